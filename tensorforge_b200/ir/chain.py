@@ -237,6 +237,8 @@ def lower(descr_list, matrix_list, global_symbols, fp: FloatingPointType) -> Cha
   for tensor, stype in global_symbols:
     if stype == 'data':
       kind = 'data'
+      if tensor.addressing not in (Addressing.SCALAR,) and tensor.data is None:
+        kind = 'batched'
     elif stype == 'scalar':
       kind = 'scalar'
     elif tensor.addressing == Addressing.NONE:

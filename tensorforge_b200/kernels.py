@@ -1,0 +1,59 @@
+"""Named kernel configurations built ahead of time (tests, smoke, benchmark).
+
+Each entry is a Generator for a chain from the case catalogue with a given precision /
+strategy. `build()` in __graft_entry__ compiles all of them so that the GPU machine
+only loads prebuilt libraries.
+"""
+from .common.basic_types import FloatingPointType
+from .common.context import Context, Options
+from .generators.generator import Generator
+
+FP = {'float': FloatingPointType.FLOAT, 'double': FloatingPointType.DOUBLE}
+
+# (case, fp, options kwargs) beyond the golden-vector cases
+EXTRA = [
+  ('chain_o6', 'float', {}),
+  ('chain_o6', 'float', {'variant': {'strategy': 'generic'}}),
+  ('chain_o6', 'float', {'precision': 'tf32x3'}),
+  ('chain_o6', 'float', {'precision': 'fp16x3'}),
+  ('chain_o6', 'float', {'precision': 'bf16x3'}),
+  ('chain_o6', 'double', {}),
+  ('chain_o6', 'double', {'precision': 'dmma'}),
+  ('c0_gemm_ptr', 'float', {}),
+]
+
+
+def make(case, fp='float', **opts):
+  from oracle import cases  # the case catalogue is shared with the tests
+  ns = cases.ns_from_module('tensorforge_b200')
+  g = Generator(cases.build(case, ns), Context('sm_100a', 'cuda', FP[fp], Options(**opts)))
+  g.generate()
+  return g
+
+
+def catalogue():
+  import glob
+  import json
+  import os
+  import numpy as np
+  root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+  out, seen = [], set()
+
+  def add(case, fp, opts):
+    key = (case, fp, json.dumps(opts, sort_keys=True))
+    if key in seen:
+      return
+    seen.add(key)
+    try:
+      out.append((f'{case}/{fp}/{key[2]}', make(case, fp, **opts)))
+    except Exception:  # a variant that does not apply to this chain is skipped
+      if not opts:
+        raise
+
+  for path in sorted(glob.glob(os.path.join(root, 'tests', 'golden', '*.npz'))):
+    meta = json.loads(bytes(np.load(path)['meta']).decode())
+    add(meta['case'], meta['fp'], {})
+    add(meta['case'], meta['fp'], {'variant': {'strategy': 'generic'}})
+  for case, fp, opts in EXTRA:
+    add(case, fp, opts)
+  return out

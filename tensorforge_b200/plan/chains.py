@@ -1,0 +1,175 @@
+"""Shared-left GEMM chains: recognition and plans for the fast generators.
+
+A chain qualifies when it computes, for every batch element e,
+
+    out_e  (+)=  sum_t  A_t * B_{e,t} * R_{e,t}
+
+with A_t shared across the batch (Addressing.NONE, dense or sparse), B_{e,t} batched and
+dense, R_{e,t} batched or shared (dense or sparse) or absent, written in the
+reference's descriptor form (tensorforge/generators/descriptions.py:14-27):
+
+    T_t  =  A_t x B_t            (temporary, targets [[0,-1],[-1,1]])
+    out (+)= T_t x R_t           (targets [[0,-1],[-1,1]], add for t > 0)
+
+or a single `out (+)= A x B`. All operands must span their full shape (bounding box =
+shape) so that columns are contiguous. This is the shape of BASELINE configs 0-3
+(benchmarks/fused/programs/s3time.cf) and of SeisSol's volume/local kernels.
+"""
+from dataclasses import dataclass
+from typing import List, Optional
+
+from ..common.basic_types import DataFlowDirection
+from . import Plan, SMEM_LIMIT
+
+
+@dataclass
+class Term:
+  A: object          # Operand (shared)
+  B: object          # Operand (batched, dense)
+  R: Optional[object]  # Operand (batched/shared) or None
+  K: int
+  P: int
+
+
+@dataclass
+class LeftChain:
+  terms: List[Term]
+  out: object
+  M: int
+  N: int
+  accumulate: bool   # out_e += ... (previous value read once)
+
+
+def _full(op):
+  t = op.tensor
+  return list(t.bbox.lower()) == [0] * len(t.shape) and list(t.bbox.upper()) == list(t.shape)
+
+
+def _full_ref(stage, ref):
+  box = [stage.n_ranges[x] if x >= 0 else stage.k_ranges[-x - 1] for x in ref.target]
+  return [l for l, _ in box] == [0] * len(box) and [u for _, u in box] == list(ref.op.shape)
+
+
+def match_left_chain(chain) -> Optional[LeftChain]:
+  st = chain.stages
+  if not st:
+    return None
+  for s in st:
+    if not s.is_matmul():
+      return None
+    for r in s.ops:
+      if r.op.kind == 'tmp':
+        continue
+      if r.op.kind not in ('shared', 'batched') or not _full(r.op) or not _full_ref(s, r):
+        return None
+  out = None
+  terms = []
+  i = 0
+  accumulate = False
+  while i < len(st):
+    s = st[i]
+    if s.dest.kind == 'tmp':
+      if i + 1 >= len(st):
+        return None
+      s2 = st[i + 1]
+      a, b = s.ops
+      t, r = s2.ops
+      if t.op is not s.dest or s2.dest.kind != 'batched' or s.add:
+        return None
+      if r.op.kind == 'tmp':
+        return None
+      if a.op.kind != 'shared' or b.op.kind != 'batched' or b.op.sparse:
+        return None
+      # the temporary must not be used anywhere else
+      if sum(1 for x in st for y in x.ops if y.op is s.dest) != 1:
+        return None
+      dest = s2.dest
+      term = Term(a.op, b.op, r.op, a.op.shape[1], b.op.shape[1])
+      add = s2.add
+      i += 2
+    else:
+      if s.dest.kind != 'batched':
+        return None
+      a, b = s.ops
+      if a.op.kind != 'shared' or b.op.kind != 'batched' or b.op.sparse:
+        return None
+      dest = s.dest
+      term = Term(a.op, b.op, None, a.op.shape[1], b.op.shape[1])
+      add = s.add
+      i += 1
+    if dest.sparse or not _full(dest):
+      return None
+    if out is None:
+      out = dest
+      accumulate = add
+    elif dest is not out or not add:
+      return None
+    terms.append(term)
+  M, N = out.shape
+  for t in terms:
+    if t.A.shape[0] != M or t.B.shape[0] != t.K:
+      return None
+    if t.R is None and t.P != N:
+      return None
+    if t.R is not None and (t.R.shape[0] != t.P or t.R.shape[1] != N):
+      return None
+    if t.B is out or t.A is out or t.R is out:
+      return None
+  return LeftChain(terms, out, M, N, accumulate)
+
+
+def a_values(term):
+  """Consumption order of A_t's nonzeros: column l outer, row i inner.
+
+  Returns [(l, [(i, storage position), ...]), ...] for l = 0..K-1.
+  """
+  A = term.A
+  M, K = A.shape
+  if A.sparse:
+    look = A.sparse_lookup()
+    cols = []
+    for l in range(K):
+      rows = [(i, look[(i, l)]) for i in range(M) if (i, l) in look]
+      cols.append((l, rows))
+    return cols
+  return [(l, [(i, l * M + i) for i in range(M)]) for l in range(K)]
+
+
+def r_slots(term):
+  """Per output column j: [(m, storage position)] of R_t's nonzeros in column j."""
+  R = term.R
+  P, N = R.shape
+  if R.sparse:
+    look = R.sparse_lookup()
+    return [[(m, look[(m, j)]) for m in range(P) if (m, j) in look] for j in range(N)]
+  return [[(m, j * P + m) for m in range(P)] for j in range(N)]
+
+
+def colprog_plan(chain, shape: LeftChain, fp_size, variant):
+  threads = variant.get('threads', 128)
+  chunk = variant.get('chunk')
+  kmax = max(t.K for t in shape.terms)
+  if chunk is None:
+    chunk = kmax if kmax <= 32 else (28 if shape.M <= 64 else 16)
+  vec = 4 if fp_size == 4 else 2
+  a_vals = 0
+  for t in shape.terms:
+    n = sum(len(rows) for _, rows in a_values(t))
+    a_vals += (n + vec - 1) // vec * vec
+  slot_entries = sum(sum(len(c) for c in r_slots(t)) for t in shape.terms if t.R is not None)
+  smem = a_vals * fp_size + 8 * (slot_entries + shape.N * len(shape.terms) + 4)
+  if smem > SMEM_LIMIT:
+    return None
+  if shape.M > 128:
+    return None
+  return Plan('colprog', {'threads': threads, 'chunk': chunk, 'min_blocks': variant.get('min_blocks', 0)},
+              smem, threads, note=f'M={shape.M} N={shape.N} terms={len(shape.terms)}')
+
+
+def tcsplit_plan(chain, shape, precision, variant):
+  from ..codegen import tcsplit
+  return tcsplit.plan(chain, shape, precision, variant)
+
+
+def dmma_plan(chain, shape, variant):
+  return None
