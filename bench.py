@@ -1,0 +1,398 @@
+"""Benchmark: fused order-6 volume chain, elements/s on B200 (one JSON line on rank 0).
+
+Workload: out_e(56x9) = sum_{t=0..2} K_t(56x56) * Q_e(56x9) * S_{e,t}(9x9),
+K_t shared and sparse (seeded Bernoulli(0.45) pattern, ~1411 nonzeros), S_{e,t} per
+element with 24 seeded nonzeros stored compactly at the start of a strided 81-value slot,
+Q/out strided, uniform[-1,1] synthetic values, 500,000 elements per GPU (inputs of 2.2 GB,
+larger than L2, so no flush is needed between steps). One step = one launch of the
+generated kernel over all elements. The chain is generated through the public frontend
+(`Generator`) and called through the emitted C-ABI launcher.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--variant auto|plain|tf32x3|fp16x3|bf16x3] [--elements E]
+
+For N > 1 the driver launches one process per GPU (torchrun); elements are independent, so
+each rank runs its own 500,000 elements (weak scaling) with no collective on the data
+path; the time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = 'order-6 chain elements/s: split-TC vs plain FP32, same B200, rel err≤1e-6'
+CASE = 'chain_o6'
+FALLBACK_HBM = 6650.0
+
+
+def log(*a):
+  print(*a, file=sys.stderr, flush=True)
+
+
+def peaks():
+  path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+  if os.path.exists(path):
+    with open(path) as f:
+      p = json.load(f)
+    return p, 'measured'
+  return {'hbm_gbs': FALLBACK_HBM, 'bf16_tflops': 1590.0}, 'fallback'
+
+
+class Clocks:
+  """nvidia-smi sampler over the timed region."""
+
+  def __init__(self, index=0):
+    self.index = index
+    self.proc = None
+    self.path = os.path.join(ROOT, 'gpurun_out', f'clocks_{os.getpid()}.csv')
+
+  def __enter__(self):
+    os.makedirs(os.path.dirname(self.path), exist_ok=True)
+    q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+         'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+         'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+    try:
+      self.f = open(self.path, 'w')
+      self.proc = subprocess.Popen(['nvidia-smi', f'--id={self.index}', f'--query-gpu={q}',
+                                    '--format=csv,noheader,nounits', '-lms', '100'],
+                                   stdout=self.f, stderr=subprocess.DEVNULL)
+      time.sleep(0.3)
+    except (OSError, FileNotFoundError):
+      self.proc = None
+    return self
+
+  def __exit__(self, *a):
+    if self.proc is not None:
+      time.sleep(0.2)
+      self.proc.terminate()
+      self.proc.wait()
+      self.f.close()
+
+  def summary(self):
+    if self.proc is None or not os.path.exists(self.path):
+      return None
+    mhz, mx, reasons = [], 0, set()
+    names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+    for line in open(self.path):
+      p = [x.strip() for x in line.split(',')]
+      if len(p) < 9:
+        continue
+      try:
+        mhz.append(float(p[1]))
+        mx = max(mx, float(p[2]))
+      except ValueError:
+        continue
+      for n, v in zip(names, p[5:9]):
+        if v.lower() == 'active':
+          reasons.add(n)
+    if not mhz:
+      return None
+    return {'sm_mhz': statistics.median(mhz), 'sm_max_mhz': mx, 'reasons': sorted(reasons), 'samples': len(mhz)}
+
+
+# ----------------------------------------------------------------------------- data
+
+def make_inputs(gen, n, device, seed):
+  """Device buffers in the launcher's ABI layout for the order-6 chain."""
+  import torch
+  g = torch.Generator(device=device)
+  g.manual_seed(seed)
+  bufs = {}
+  for t, stype in gen.abi_symbols():
+    if t.addressing.name == 'NONE':
+      size = t.spp.count_nz()
+      bufs[t.name] = torch.rand(size, generator=g, device=device) * 2 - 1
+    else:
+      vol = t.get_real_volume()
+      bufs[t.name] = torch.rand(n * vol, generator=g, device=device) * 2 - 1
+  return bufs
+
+
+def check_accuracy(descrs, gen, bufs, n_check):
+  """Relative-L2 and max-abs error of the first n_check elements vs the FP64 oracle."""
+  import numpy as np
+  from oracle.multilinear import Memory, evaluate
+  mem = Memory()
+  outname = None
+  for t, _ in gen.abi_symbols():
+    b = bufs[t.name]
+    if t.addressing.name == 'NONE':
+      mem.buffers[t.name] = b.double().cpu().numpy()
+      continue
+    vol = t.get_real_volume()
+    mem.buffers[t.name] = b[:n_check * vol].double().cpu().numpy().copy()
+    mem.starts[t.name] = np.arange(n_check, dtype=np.int64) * vol
+    if t.direction.name != 'SOURCE':
+      outname = t.name
+  got = mem.buffers[outname].copy()
+  evaluate(descrs, mem, n_check)
+  ref = mem.buffers[outname]
+  rel = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+  return {'rel_l2': rel, 'max_abs': float(np.abs(got - ref).max()), 'ref_max_abs': float(np.abs(ref).max()),
+          'elements_checked': n_check}
+
+
+def time_launches(fn, stream, steps, warmup, dist=None):
+  """Run warmup untimed steps, then `steps` timed ones; per-launch and total times (ms)."""
+  import torch
+  for _ in range(warmup):
+    fn()
+  torch.cuda.synchronize()
+  if dist is not None:
+    dist.barrier()
+  torch.cuda.synchronize()
+  evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+  t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+  t0.record(stream)
+  for s, e in evs:
+    s.record(stream)
+    fn()
+    e.record(stream)
+  t1.record(stream)
+  torch.cuda.synchronize()
+  if dist is not None:
+    dist.barrier()
+  torch.cuda.synchronize()
+  per = [s.elapsed_time(e) for s, e in evs]
+  return t0.elapsed_time(t1), per
+
+
+# ----------------------------------------------------------------------------- CPU baseline
+
+def _cpu_bench(args_list):
+  """Run oracle/cpu_bench.py in a fresh interpreter (system OpenMP runtime) and parse its JSON."""
+  cmd = [sys.executable, '-m', 'oracle.cpu_bench'] + args_list
+  env = dict(os.environ)
+  env.setdefault('OMP_TARGET_OFFLOAD', 'DISABLED')
+  proc = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, env=env, timeout=900)
+  if proc.returncode != 0:
+    log(proc.stderr[-2000:])
+    return None
+  return json.loads(proc.stdout.strip().splitlines()[-1])
+
+
+def reference_cpu(n_target_s=8.0):
+  """The reference's OpenMP-backend chain kernel on all host cores, bounded sample."""
+  from oracle import baseline
+  tag = 'bench_chain_o6_float'
+  if not baseline.available(tag):
+    return None
+  r = _cpu_bench(['--tag', tag, '--case', CASE, '--seconds', str(n_target_s)])
+  if r is None:
+    return None
+  return {'value': r['elements_per_s'], 'unit': 'elements/s', 'cores': r['cores'], 'kind': 'reference',
+          'sample': f'{r["elements"]} elements of the 500,000-element workload, one call of the reference '
+                    f'OpenMP-backend kernel (g++ -O3 -march=native -fopenmp, host fallback), '
+                    f'{r["times"][0]:.1f} s'}
+
+
+def impl_reference(args, rank, world):
+  if rank != 0:
+    return
+  from oracle import baseline
+  tag = 'bench_chain_o6_float'
+  if not baseline.available(tag):
+    print(json.dumps({'impl': 'reference', 'unavailable': 'reference OpenMP build missing (oracle/_ref)'}))
+    return
+  n = args.ref_sample
+  r = _cpu_bench(['--tag', tag, '--case', CASE, '--fixed', str(n), '--steps', str(args.steps),
+                  '--warmup', str(args.warmup)])
+  if r is None:
+    print(json.dumps({'impl': 'reference', 'unavailable': 'reference OpenMP kernel failed to run'}))
+    return
+  ms = 1e3 * sum(r['times']) / len(r['times'])
+  value = r['elements_per_s']
+  line = {
+    'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': 'elements/s', 'n_gpus': world,
+    'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True,
+    'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+    'config': {'workload': 'order-6 volume chain 56x9, 3 terms, K 45% sparse, S 24 nnz, FP32',
+               'elements_per_step': n, 'full_workload_elements': args.elements},
+    'cpu_baseline': {'value': value, 'unit': 'elements/s', 'cores': r['cores'], 'kind': 'reference',
+                     'sample': f'{n} elements per step (bounded sample of the {args.elements}-element workload), '
+                               'reference OpenMP-backend kernel on all host threads'},
+    'e2e': {'value': value, 'unit': 'elements/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+  }
+  print(json.dumps(line))
+
+
+# ----------------------------------------------------------------------------- ours
+
+def impl_ours(args, rank, world, dist):
+  import torch
+  from oracle import cases
+  from tensorforge_b200.kernels import make
+  from tensorforge_b200.runtime import compile_generator
+  from tensorforge_b200.common.basic_types import DataFlowDirection
+  device = torch.device('cuda', torch.cuda.current_device())
+  n = args.elements
+  variants = ['plain'] if args.variant == 'plain' else (
+    [args.variant] if args.variant != 'auto' else ['tf32x3', 'fp16x3', 'plain'])
+  opts_of = {'plain': {}, 'tf32x3': {'precision': 'tf32x3'}, 'fp16x3': {'precision': 'fp16x3'},
+             'bf16x3': {'precision': 'bf16x3'}, 'generic': {'variant': {'strategy': 'generic'}}}
+  results = {}
+  stream = torch.cuda.current_stream()
+  primary = None
+  ref_gen = make(CASE, 'float')
+  bufs = make_inputs(ref_gen, n, device, seed=1234 + rank)
+  outname = [t.name for t, _ in ref_gen.abi_symbols() if t.direction != DataFlowDirection.SOURCE][0]
+  descrs = cases.build(CASE, cases.ns_from_module('tensorforge_b200'))
+  extra = ['plain'] if 'plain' not in variants else []
+  for name in variants + extra:
+    try:
+      gen = make(CASE, 'float', **opts_of[name])
+    except Exception as e:  # variant not available for this chain
+      log(f'variant {name} unavailable: {e}')
+      continue
+    if name != 'plain' and gen.get_plan().strategy == 'colprog':
+      log(f'variant {name} fell back to {gen.get_plan().strategy}; skipped')
+      continue
+    k = compile_generator(gen)
+    kw = {t.name: bufs[t.name] for t, _ in gen.abi_symbols()}
+    kw['numElements'] = n
+    kw['streamPtr'] = stream.cuda_stream
+    fn = lambda k=k, kw=kw: k(**kw)  # noqa: E731
+    fn()
+    torch.cuda.synchronize()
+    acc = check_accuracy(descrs, gen, bufs, min(n, 2048))
+    steps = args.steps if primary is None else max(3, args.steps // 2)
+    total, per = time_launches(fn, stream, steps, max(3, args.warmup), dist if primary is None else None)
+    results[name] = {'kernel': gen.get_base_name(), 'plan': gen.get_plan().key(), 'ms_total': total,
+                     'launch_ms': per, 'accuracy': acc, 'gen': gen, 'k': k, 'kw': kw}
+    ok = name == 'plain' or acc['rel_l2'] <= 1e-6
+    if primary is None and ok:
+      primary = name
+    log(f'{name}: {n / (total / steps / 1e3):.3e} el/s, rel_l2 {acc["rel_l2"]:.2e}, plan {gen.get_plan().key()}')
+  if primary is None:
+    raise RuntimeError('no benchmark variant ran')
+  pr = results[primary]
+  k, kw, gen = pr['k'], pr['kw'], pr['gen']
+
+  # the timed region of record: K steps of the primary variant, clocks sampled meanwhile
+  with Clocks(index=torch.cuda.current_device()) as clocks:
+    total, per = time_launches(lambda: k(**kw), stream, args.steps, args.warmup, dist)
+  ms = total / args.steps
+  if dist is not None:
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+  value = world * n / (ms / 1e3)
+
+  # end to end through the C-ABI launcher with host buffers (pinned), copies inside the timed region
+  host = {name: b.cpu().pin_memory() for name, b in bufs.items()}
+  inputs = [t.name for t, _ in gen.abi_symbols() if t.direction == DataFlowDirection.SOURCE]
+  h2d = sum(host[x].numel() * host[x].element_size() for x in inputs)
+  d2h = host[outname].numel() * host[outname].element_size()
+
+  def e2e_step():
+    for x in inputs:
+      kw[x].copy_(host[x], non_blocking=True)
+    k(**kw)
+    host[outname].copy_(kw[outname], non_blocking=True)
+
+  e_steps = max(2, min(args.steps, 5))
+  e_total, _ = time_launches(e2e_step, stream, e_steps, 1, dist)
+  e_ms = e_total / e_steps
+  if dist is not None:
+    t = torch.tensor([e_ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e_ms = float(t.item())
+
+  if rank != 0:
+    return
+  chain = gen.get_chain()
+  bytes_el = chain.bytes_per_element()
+  shared_bytes = sum(o.storage_size() * 4 for o in chain.shared())
+  alg_bytes = n * bytes_el + shared_bytes
+  mean_launch = sum(per) / len(per)
+  pk, pk_src = peaks()
+  achieved = alg_bytes / (mean_launch / 1e3) / 1e9
+  traffic = None
+  prof = os.path.join(ROOT, 'profiles', f'traffic_{pr["kernel"]}.json')
+  if os.path.exists(prof):
+    with open(prof) as f:
+      tr = json.load(f)
+    traffic = tr.get('bytes_per_element', 0) * n + shared_bytes if 'bytes_per_element' in tr else tr.get('traffic')
+  roofline = {'bound': 'hbm', 'achieved': achieved, 'peak': pk['hbm_gbs'], 'unit': 'GB/s',
+              'frac': achieved / pk['hbm_gbs'], 'traffic': traffic,
+              'peak_source': f'{pk_src} HBM copy bandwidth', 'kernel': pr['kernel'],
+              'algorithmic_bytes_per_launch': alg_bytes}
+  nz = chain.nz_flops_per_element()
+  plain = results.get('plain')
+  extra_out = {}
+  if plain is not None:
+    p_launch = sum(plain['launch_ms']) / len(plain['launch_ms'])
+    from tensorforge_b200.runtime.peaks import fma_peak
+    fp32_peak = fma_peak('float')
+    p_flops = n * nz / (p_launch / 1e3)
+    extra_out['plain_fp32'] = {
+      'elements_per_s': n / (p_launch / 1e3), 'kernel': plain['kernel'], 'plan': plain['plan'],
+      'accuracy': plain['accuracy'],
+      'roofline': {'bound': 'fp32', 'achieved': p_flops / 1e12, 'peak': fp32_peak / 1e12, 'unit': 'TFLOP/s',
+                   'frac': p_flops / fp32_peak, 'flops_per_element': nz,
+                   'peak_source': 'measured FP32 FFMA probe (libtfb200_runtime tfb_fma_peak_launch), same run'}}
+  for name, r in results.items():
+    extra_out.setdefault('variants', {})[name] = {
+      'elements_per_s': n / (sum(r['launch_ms']) / len(r['launch_ms']) / 1e3), 'plan': r['plan'],
+      'rel_l2': r['accuracy']['rel_l2'], 'max_abs': r['accuracy']['max_abs']}
+  cpu = reference_cpu() if (world == 1 and not args.no_cpu) else None
+  line = {
+    'metric': METRIC, 'value': value, 'unit': 'elements/s', 'n_gpus': world, 'steps': args.steps,
+    'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
+    'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+    'config': {'workload': 'order-6 volume chain: out(56x9) = sum_3 K(56x56, 45% sparse) Q(56x9) S(9x9, 24 nnz), FP32',
+               'elements_per_gpu': n, 'variant': primary, 'plan': pr['plan'],
+               'l2': 'inputs larger than L2 (no flush)'},
+    'accuracy': pr['accuracy'],
+    'roofline': roofline,
+    'cpu_baseline': cpu,
+    'e2e': {'value': world * n / (e_ms / 1e3), 'unit': 'elements/s', 'h2d_bytes_per_step': h2d,
+            'd2h_bytes_per_step': d2h},
+    'gpu_launches': args.steps,
+    'clocks': clocks.summary(),
+  }
+  line.update(extra_out)
+  print(json.dumps(line))
+
+
+def main():
+  ap = argparse.ArgumentParser()
+  ap.add_argument('--gpus', type=int, default=1)
+  ap.add_argument('--steps', type=int, default=20)
+  ap.add_argument('--warmup', type=int, default=5)
+  ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+  ap.add_argument('--variant', default='auto')
+  ap.add_argument('--elements', type=int, default=500000)
+  ap.add_argument('--ref-sample', type=int, default=4096)
+  ap.add_argument('--no-cpu', action='store_true')
+  args = ap.parse_args()
+  rank = int(os.environ.get('RANK', '0'))
+  world = int(os.environ.get('WORLD_SIZE', '1'))
+  if args.impl == 'reference':
+    impl_reference(args, rank, world)
+    return
+  import torch
+  dist = None
+  if world > 1:
+    import datetime
+    import torch.distributed as tdist
+    torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', '0')))
+    tdist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+    dist = tdist
+  else:
+    torch.cuda.set_device(0)
+  try:
+    impl_ours(args, rank, world, dist)
+  finally:
+    if dist is not None:
+      dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+  main()

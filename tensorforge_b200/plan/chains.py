@@ -150,7 +150,8 @@ def colprog_plan(chain, shape: LeftChain, fp_size, variant):
   chunk = variant.get('chunk')
   kmax = max(t.K for t in shape.terms)
   if chunk is None:
-    chunk = kmax if kmax <= 32 else (28 if shape.M <= 64 else 16)
+    chunk = kmax if kmax <= 16 else 16
+  chunk = max(4, (chunk + 3) // 4 * 4)
   vec = 4 if fp_size == 4 else 2
   a_vals = 0
   for t in shape.terms:
