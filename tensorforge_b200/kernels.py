@@ -15,8 +15,8 @@ EXTRA = [
   ('chain_o6', 'float', {}),
   ('chain_o6', 'float', {'variant': {'strategy': 'generic'}}),
   ('chain_o6', 'float', {'precision': 'tf32x3'}),
-  ('chain_o6', 'float', {'precision': 'fp16x3'}),
   ('chain_o6', 'float', {'precision': 'bf16x3'}),
+  ('chain_o4_q27', 'float', {'precision': 'tf32x3'}),
   ('chain_o6', 'double', {}),
   ('chain_o6', 'double', {'precision': 'dmma'}),
   ('c0_gemm_ptr', 'float', {}),

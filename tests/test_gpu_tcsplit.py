@@ -1,0 +1,78 @@
+"""GPU: tcgen05 split-precision chains vs the FP64 oracle and the plain FP32 path.
+
+Tolerances (relative L2 over the whole output, the reference test suite's norm):
+TF32x3 <= 1e-6 (the order-6 target), BF16x3 <= 5e-5 (16 significant bits per product).
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import cases, harness, multilinear
+
+pytestmark = pytest.mark.gpu
+
+TOL = {'tf32x3': 1e-6, 'bf16x3': 5e-5}
+
+
+def _run(case, precision, n, seed=3, dist='uniform', use_flags=False):
+  import torch
+  from tensorforge_b200.kernels import make
+  from tensorforge_b200.runtime import compile_generator
+  g = make(case, 'float', precision=precision)
+  assert g.get_plan().strategy == 'tcsplit', g.get_plan()
+  k = compile_generator(g)
+  descrs = cases.build(case, cases.ns_from_module('tensorforge_b200'))
+  lay, mem = harness.make_memory(descrs, n, seed=seed, dist=dist)
+  flags = harness.make_flags(n, seed) if use_flags else None
+  dev, kw = {}, {'numElements': n}
+  for l in lay:
+    dev[l.name] = torch.tensor(mem.buffers[l.name], dtype=torch.float32, device='cuda')
+    kw[l.name] = dev[l.name]
+    if l.kind == 'strided':
+      kw[f'{l.name}_extraOffset'] = l.extra_offset
+  if flags is not None:
+    kw['flags'] = torch.tensor(flags, dtype=torch.int32, device='cuda')
+  k(**kw)
+  torch.cuda.synchronize()
+  lib = ctypes.CDLL(k.so_path)
+  errf = getattr(lib, f'tfb_kernel_error_{g.get_base_name()}')
+  errf.argtypes = [ctypes.c_void_p]
+  assert errf(None) == 0
+  # oracle on float32-exact inputs
+  multilinear.evaluate(descrs, mem, n, flags=flags)
+  out = [l for l in lay if l.kind == 'strided' and l.tensor.direction.name != 'SOURCE'][0]
+  got = dev[out.name].double().cpu().numpy()
+  ref = mem.buffers[out.name]
+  return got, ref, out, flags
+
+
+@pytest.mark.parametrize('precision', ['tf32x3', 'bf16x3'])
+@pytest.mark.parametrize('n', [1, 14, 333, 4099])
+def test_chain_o6_split(precision, n):
+  got, ref, out, _ = _run('chain_o6', precision, n)
+  rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+  assert rel <= TOL[precision], rel
+
+
+def test_chain_o6_flags_mask_elements():
+  got, ref, out, flags = _run('chain_o6', 'tf32x3', 517, use_flags=True)
+  rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+  assert rel <= 1e-6
+  # masked elements keep their previous contents exactly (the oracle leaves them untouched)
+  for e in np.nonzero(flags == 0)[0][:5]:
+    s = out.starts[e]
+    assert np.array_equal(got[s:s + 504], ref[s:s + 504])
+
+
+def test_chain_o6_loguniform_tf32x3():
+  """Values with magnitudes spanning 1e-3..1e3 (precision-form inputs)."""
+  got, ref, _, _ = _run('chain_o6', 'tf32x3', 777, dist='loguniform')
+  rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+  assert rel <= 1e-6, rel
+
+
+def test_other_shapes_split():
+  got, ref, _, _ = _run('chain_o4_q27', 'tf32x3', 301)
+  rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+  assert rel <= 1e-6, rel
