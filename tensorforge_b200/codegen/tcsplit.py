@@ -4,35 +4,46 @@ Computes out_e = sum_t A_t * B_{e,t} * R_{e,t} (the chains of plan.chains) as
 
     out^T[(e,j), i] = sum_t sum_l U_t[l, (e,j)] * A_t[i, l],   U_t = B_{e,t} * R_{e,t}
 
-i.e. one MMA chain per tile of 128 flat output columns (e, j):
-  * M = 128 flat columns (one TMEM lane each), N = rows of out padded to 16,
+one MMA chain per tile of TE = floor(128 / N) whole elements (TE*N flat output columns):
+  * M = 128 rows = flat columns (e, j) (one TMEM lane each), N = rows of out padded to 16,
     K = sum_t K_t (each term padded to the MMA K step);
-  * A operand (U^T, per element) lives in tensor memory: lane c's producer thread computes
-    column j of U_t = B_e * R_t on CUDA cores (the column program of codegen/colprog.py),
-    splits it into hi + lo and writes both with tcgen05.st;
+  * A operand (U^T, per element) lives in tensor memory. Per tile, the batched operands
+    are prefetched one tile ahead into a double-buffered shared-memory stage with
+    cp.async (coalesced 16-byte chunks); one producer thread per (element, row l)
+    computes row l of U_t = B_e * R_{e,t} for all j with R_t's compile-time pattern
+    unrolled and writes it to a padded transposition buffer; then each lane reads its
+    column (e, j), splits it into hi + lo and writes both with tcgen05.st;
   * B operand (A_t^T, shared) is split once per CTA into hi + lo and kept in shared memory
     in the canonical no-swizzle K-major layout (8x16-byte core matrices);
-  * D accumulates in tensor memory in FP32 over the three split products
-    hi*hi + hi*lo + lo*hi (the lo*lo term is below FP32 resolution); the producer lane
-    then reads its output column with tcgen05.ld and stores it contiguously.
+  * the epilogue reads the accumulators with tcgen05.ld, stages the tile's output in
+    shared memory and writes it with one bulk copy (cp.async.bulk, shared -> global) when
+    the output is strided, 16-byte aligned and unmasked; otherwise each lane stores its
+    own column.
 
-Precisions: 'tf32x3' (kind::tf32: hi = value with the 13 low mantissa bits cleared, so
-it is exact in TF32, lo = value - hi), 'bf16x3' (kind::f16 with BF16 inputs: hi =
-bf16(value), lo = bf16(value - hi)). TF32x3 keeps ~22 significant bits per product;
-BF16x3 keeps ~16 (relative error ~1e-5, reported, not used where 1e-6 is required).
+Precisions: 'tf32x3' (kind::tf32: hi = value rounded to nearest TF32, lo = the rounded
+remainder, so value = hi + lo to ~2^-24 and both are exact TF32 inputs), 'bf16x3'
+(kind::f16 with BF16 inputs: hi = bf16(value), lo = bf16(value - hi); ~16 significant
+bits, relative error ~1e-5, reported, not used where 1e-6 is required).
 
-Pipelining: A has one TMEM slot per term and D two buffers; mbarriers hand slots between
-the 4 producer warps and the MMA-issuing thread, so the tensor cores work on tile n while
-the producers compute tile n+1 and store tile n-1. Every mbarrier wait is bounded: on
-timeout the kernel records an error code (read with tfb_kernel_error_<name>) and exits
-after releasing its tensor memory.
+Accumulation: hi*hi products accumulate in one TMEM accumulator and the cross terms
+hi*lo + lo*hi in a second one; the epilogue adds them in FP32. Every tensor-core
+accumulation step rounds relative to its accumulator, so keeping the small cross terms
+apart cuts the rounding error on the output by the share of MMAs they account for (2/3).
+
+Pipelining: A has one TMEM slot per term; mbarriers hand slots between the producer warps
+(4 groups of 4 warps sharing the 4 TMEM lane quadrants) and the MMA-issuing thread, so
+the tensor cores work on tile n while the producers compute tile n+1; tile n's epilogue
+then frees the accumulators for tile n+1. Every mbarrier wait is bounded: on timeout the
+kernel records an error code (read with tfb_kernel_error_<name>) and exits after
+releasing its tensor memory.
 """
 from .. import plan as _plan
 from ..plan import Plan
-from ..plan.chains import match_left_chain, a_values, r_slots
+from ..plan.chains import match_left_chain
 
 KSTEP = {'tf32x3': 8, 'bf16x3': 16}
 ESIZE = {'tf32x3': 4, 'bf16x3': 2}
+H_GROUPS = 4
 
 
 def _pad(x, m):
@@ -46,27 +57,60 @@ def layout(shape, precision):
   kpad = [_pad(t.K, ks) for t in shape.terms]
   a_cols = [kp * es // 4 for kp in kpad]          # TMEM columns per split per term
   slot_cols = [2 * c for c in a_cols]               # hi + lo
-  tmem_used = sum(slot_cols) + 2 * n_mma
+  tmem_used = sum(slot_cols) + 2 * n_mma            # + main and correction accumulators
   b_bytes = sum(2 * n_mma * kp * es for kp in kpad)  # hi + lo, all terms
+  te = 128 // shape.N if shape.N <= 128 else 0
   return dict(ks=ks, es=es, n_mma=n_mma, kpad=kpad, a_cols=a_cols, slot_cols=slot_cols,
-              tmem_used=tmem_used, b_bytes=b_bytes)
+              tmem_used=tmem_used, b_bytes=b_bytes, te=te)
+
+
+def staged_operands(shape):
+  """Distinct batched operands a tile stages: [(operand, values per element)]."""
+  seen = []
+  for t in shape.terms:
+    for op, vals in ((t.B, t.B.element_volume()), (t.R, t.R.storage_size() if t.R is not None else 0)):
+      if op is None or op.kind != 'batched':
+        continue
+      if all(op is not o for o, _ in seen):
+        seen.append((op, vals))
+  return seen
+
+
+def smem_plan(shape, precision):
+  lay = layout(shape, precision)
+  te = lay['te']
+  tc = te * shape.N
+  stage = sum(te * _pad(v, 4) * 4 for _, v in staged_operands(shape))
+  kmax = max(t.K for t in shape.terms)
+  pitch = _pad(kmax, 4) + 4
+  ubuf = max(tc * pitch * 4, tc * shape.M * 4)
+  b_bytes = lay['b_bytes']
+  off_stage = _pad(b_bytes, 128)
+  off_u = off_stage + 2 * _pad(stage, 128)
+  off_bar = off_u + _pad(ubuf, 128)
+  total = off_bar + 256
+  return dict(off_stage=off_stage, stage=_pad(stage, 128), off_u=off_u, pitch=pitch,
+              off_bar=off_bar, total=total, te=te, tc=tc)
 
 
 def plan(chain, shape, precision, variant):
   if precision not in KSTEP:
     return None
-  if shape.M > 256:
+  if shape.M > 256 or shape.N > 128:
     return None
   lay = layout(shape, precision)
-  if lay['tmem_used'] > 512:
+  if lay['tmem_used'] > 512 or lay['te'] < 1:
     return None
-  chunk = variant.get('chunk', 16 if precision == 'tf32x3' else 16)
-  smem = lay['b_bytes'] + 4096 + 8 * (sum(sum(len(c) for c in r_slots(t)) for t in shape.terms if t.R is not None) + shape.N * len(shape.terms))
-  smem = max(smem, 120 * 1024)  # one CTA per SM: it owns the SM's tensor memory
+  for t in shape.terms:
+    if t.R is not None and t.R.kind != 'batched':
+      return None
+  sm = smem_plan(shape, precision)
+  smem = max(sm['total'], 120 * 1024)  # one CTA per SM: it owns the SM's tensor memory
   if smem > _plan.SMEM_LIMIT:
     return None
-  return Plan('tcsplit', {'precision': precision, 'chunk': chunk}, smem, 160,
-              note=f'M={shape.M} N={shape.N} terms={len(shape.terms)} tmem={lay["tmem_used"]}')
+  chunk = variant.get('chunk', 16)
+  return Plan('tcsplit', {'precision': precision, 'chunk': chunk}, smem, 32 * (4 * H_GROUPS + 1),
+              note=f'M={shape.M} N={shape.N} terms={len(shape.terms)} tmem={lay["tmem_used"]} smem={sm["total"]}')
 
 
 HELPERS = r'''
@@ -97,6 +141,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsign
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void named_sync(unsigned id, unsigned n) { asm volatile("bar.sync %0, %1;" :: "r"(id), "r"(n) : "memory"); }
+// barrier over `n` threads that also returns the OR of `v` over them (same answer for all)
+__device__ __forceinline__ bool any_sync(unsigned id, unsigned n, bool v) {
+  unsigned r;
+  asm volatile("{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, %2, %3, p;\n selp.u32 %0, 1, 0, q;\n}"
+               : "=r"(r) : "r"((unsigned)v), "r"(id), "r"(n) : "memory");
+  return r != 0;
+}
 __device__ __forceinline__ void tmem_alloc(unsigned* dst_smem, unsigned ncols) {
   asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" :: "r"(smem_u32(dst_smem)), "r"(ncols) : "memory");
   asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
@@ -136,7 +188,33 @@ __device__ __forceinline__ void ld_x8(unsigned taddr, unsigned* v) {
                : "r"(taddr) : "memory");
 }
 __device__ __forceinline__ void ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-__device__ __forceinline__ unsigned tf32_hi_bits(float x) { return __float_as_uint(x) & 0xFFFFE000u; }
+// round to nearest TF32 (10 stored mantissa bits); the result is exactly representable
+__device__ __forceinline__ unsigned tf32_rna(float x) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+// x = hi + lo with both parts exactly representable in TF32 up to |x| * 2^-24
+__device__ __forceinline__ void tf32_split(float x, unsigned& hi, unsigned& lo) {
+  hi = tf32_rna(x);
+  lo = tf32_rna(x - __uint_as_float(hi));
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void bulk_store(void* gdst, const void* ssrc, unsigned bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
+               :: "l"(gdst), "r"(smem_u32(ssrc)), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 }  // namespace tfb_tc
 #endif
 '''
@@ -158,8 +236,9 @@ class _TC:
     self.base = base
     self.prec = plan_.params['precision']
     self.lay = layout(shape, self.prec)
+    self.sm = smem_plan(shape, self.prec)
     self.LC = plan_.params['chunk']
-    self.H = plan_.params.get('groups', 4)
+    self.H = H_GROUPS
     self.lines = []
     self.ind = 0
 
@@ -188,33 +267,38 @@ class _TC:
     params += ['size_t numElements', 'const unsigned* __restrict__ flags']
     return params
 
-  def _base(self, op, var):
-    const = 'const ' if op.is_const else ''
+  def _elem_ptr(self, op, e):
     a = op.addressing.name
     if a == 'STRIDED':
-      self.w(f'{const}float* const {var} = {op.name} + e * {op.element_volume()}u + {op.name}_extraOffset;')
-    elif a == 'PTR_BASED':
-      self.w(f'{const}float* const {var} = {op.name}[e] + {op.name}_extraOffset;')
-    else:
-      self.w(f'{const}float* const {var} = {op.name};')
+      return f'({op.name} + ({e}) * {op.element_volume()}u + {op.name}_extraOffset)'
+    if a == 'PTR_BASED':
+      return f'({op.name}[{e}] + {op.name}_extraOffset)'
+    return f'{op.name}'
 
+  # ------------------------------------------------------------------ emit
   def emit(self, globals_):
-    s, lay, b = self.s, self.lay, self.base
+    s, lay, sm, b = self.s, self.lay, self.sm, self.base
     kname = f'kernel_{b}'
     prec = self.prec
     n_mma = lay['n_mma']
     es = lay['es']
-    # ---------------------------------------------------------------- tables
-    # B operand (A_t^T): for every term, rows i (N, padded to n_mma) x K (padded), hi+lo,
-    # canonical no-swizzle K-major layout: (n/8)*SBO + (k/ke)*LBO + (n%8)*16 + (k%ke)*es
-    ke = 16 // es
-    b_off = []     # byte offset of (term, split) blocks in shared memory
+    H = self.H
+    NP = 128 * H                       # producer threads
+    nterms = len(s.terms)
+    te, tcols = sm['te'], sm['tc']
+    staged = staged_operands(s)
+    stage_off = {}
     off = 0
-    for ti, kp in enumerate(lay['kpad']):
+    for op, vals in staged:
+      stage_off[op.name] = off          # floats, within one stage buffer
+      off += te * _pad(vals, 4)
+    # B operand blocks (hi/lo per term) at the start of shared memory
+    ke = 16 // es
+    b_off = []
+    off = 0
+    for kp in lay['kpad']:
       b_off.append((off, off + n_mma * kp * es))
       off += 2 * n_mma * kp * es
-    b_total = off
-    # gather table: for every (term, n, k) dense element, its storage position in A_t (or -1)
     gathers = []
     for ti, t in enumerate(s.terms):
       kp = lay['kpad'][ti]
@@ -223,29 +307,14 @@ class _TC:
       for n in range(n_mma):
         for k in range(kp):
           if n < t.A.shape[0] and k < t.K:
-            if look is None:
-              tbl.append(k * t.A.shape[0] + n)
-            else:
-              tbl.append(look.get((n, k), -1))
+            tbl.append(k * t.A.shape[0] + n if look is None else look.get((n, k), -1))
           else:
             tbl.append(-1)
       gathers.append(tbl)
-    hdr, pairs, slot_hdr, slot_max = [], [], [], []
-    for t in s.terms:
-      if t.R is None:
-        slot_hdr.append(-1)
-        slot_max.append(0)
-        continue
-      sl = r_slots(t)
-      slot_hdr.append(len(hdr))
-      slot_max.append(max(len(c) for c in sl))
-      for j in range(s.N):
-        hdr.append((len(pairs), len(sl[j])))
-        for m, pos in sl[j]:
-          pairs.append((m * t.K, pos))
 
     self.w(HELPERS)
-    self.w(f'// generated by tensorforge_b200 (strategy: tcsplit, {prec}, chunk={self.LC})')
+    self.w(f'// generated by tensorforge_b200 (strategy: tcsplit, {prec}, chunk={self.LC}, '
+           f'tile={te} elements, smem={sm["total"]} B)')
     self.w('// meta data:')
     for o in self.chain.operands:
       self.w(f'// {o.tensor.gen_descr()}')
@@ -253,10 +322,6 @@ class _TC:
       self.w(f'// {st.descr}')
     for ti, tbl in enumerate(gathers):
       self.w(f'__device__ const short bgather{ti}_{b}[{len(tbl)}] = {{{", ".join(str(x) for x in tbl)}}};')
-    if hdr:
-      self.w(f'__device__ const int2 shdr_{b}[{len(hdr)}] = {{{", ".join(f"{{{x},{c}}}" for x, c in hdr)}}};')
-      self.w(f'__device__ const int2 spair_{b}[{max(1, len(pairs))}] = {{{", ".join(f"{{{x},{c}}}" for x, c in pairs) or "{0,0}"}}};')
-    self.w(f'__device__ __align__(16) const float zeros_{b}[{max(self.LC, 16) + 4}] = {{}};')
     self.w(f'__device__ unsigned tfb_err_{b} = 0u;')
     self.w(f'extern "C" int tfb_kernel_error_{b}(void* stream) {{')
     self.w('  unsigned v = 0, z = 0;')
@@ -266,68 +331,57 @@ class _TC:
     self.w('  cudaStreamSynchronize(st);')
     self.w('  return (int)v;')
     self.w('}')
-    # instruction descriptor: D f32, A/B tf32 (2) or bf16 (1), both K-major, N>>3, M>>4
     fmt = 2 if prec == 'tf32x3' else 1
     idesc = (1 << 4) | (fmt << 7) | (fmt << 10) | ((n_mma >> 3) << 17) | ((128 >> 4) << 24)
-    hdr_bytes = 8 * (len(hdr) + len(pairs))
-    bar_off = b_total + hdr_bytes
-    bar_off = (bar_off + 15) // 16 * 16
-    nterms = len(s.terms)
-    smem = max(self.plan.smem_bytes, bar_off + 16 * (2 * nterms + 4) + 64)
+    smem = max(self.plan.smem_bytes, sm['total'])
     self.plan.smem_bytes = smem
-    # TMEM column map: slot t = [hi | lo], then D0, D1
     slot_base = []
     col = 0
     for ti in range(nterms):
       slot_base.append(col)
       col += lay['slot_cols'][ti]
-    d_base = [col, col + n_mma]
+    d_main, d_corr = col, col + n_mma
     lim = self.WAIT_LIMIT
-
-    H = self.H
     nthreads = 32 * (4 * H + 1)
+    BAR_FULL, BAR_FREE, BAR_DFULL, BAR_DFREE = 0, nterms, 2 * nterms, 2 * nterms + 1
+
     self.w(f'__global__ void __launch_bounds__({nthreads}, 1) {kname}({", ".join(self.params(globals_))}) {{')
     self.ind += 1
     self.w('extern __shared__ __align__(1024) unsigned char tfb_smem_raw[];')
-    self.w(f'uint64_t* const bars = reinterpret_cast<uint64_t*>(tfb_smem_raw + {bar_off});')
-    self.w(f'// bars[0..{nterms}) afull[t], bars[{nterms}..{2 * nterms}) afree[t], bars[{2 * nterms}], [{2 * nterms + 1}] dfull[0/1]')
+    self.w(f'uint64_t* const bars = reinterpret_cast<uint64_t*>(tfb_smem_raw + {sm["off_bar"]});')
     self.w(f'unsigned* const tmem_slot = reinterpret_cast<unsigned*>(bars + {2 * nterms + 2});')
-    self.w(f'int2* const sHdr = reinterpret_cast<int2*>(tfb_smem_raw + {b_total});')
-    self.w(f'int2* const sPair = sHdr + {len(hdr)};')
+    self.w(f'float* const stage0 = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_stage"]});')
+    self.w(f'float* const stage1 = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_stage"] + sm["stage"]});')
+    self.w(f'float* const ubuf = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_u"]});')
     self.w('const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;')
-    self.w(f'const size_t totalCols = numElements * {s.N}u;')
-    self.w('const size_t numTiles = (totalCols + 127u) / 128u;')
-    # ---- setup: B operand split into smem, slot tables, barriers, TMEM
+    self.w(f'const size_t numTiles = (numElements + {te - 1}u) / {te}u;')
+    # ---- setup: B operand, barriers, TMEM
     for ti, t in enumerate(s.terms):
       kp = lay['kpad'][ti]
-      nvals = n_mma * kp
       hi_off, lo_off = b_off[ti]
       sbo = (kp // ke) * 128
-      self.open(f'for (int q = threadIdx.x; q < {nvals}; q += blockDim.x)')
+      self.open(f'for (int q = threadIdx.x; q < {n_mma * kp}; q += blockDim.x)')
       self.w(f'const int n = q / {kp}, k = q - n * {kp};')
       self.w(f'const int src = bgather{ti}_{b}[q];')
       self.w(f'const float v = src >= 0 ? {t.A.name}[src] : 0.0f;')
       self.w(f'const unsigned boff = (n >> 3) * {sbo}u + (k / {ke}) * 128u + (n & 7) * 16u + (k % {ke}) * {es}u;')
       if prec == 'tf32x3':
-        self.w('const unsigned hb = tfb_tc::tf32_hi_bits(v);')
-        self.w('const float lo = v - __uint_as_float(hb);')
+        self.w('unsigned hb, lb;')
+        self.w('tfb_tc::tf32_split(v, hb, lb);')
         self.w(f'*reinterpret_cast<unsigned*>(tfb_smem_raw + {hi_off} + boff) = hb;')
-        self.w(f'*reinterpret_cast<float*>(tfb_smem_raw + {lo_off} + boff) = lo;')
+        self.w(f'*reinterpret_cast<unsigned*>(tfb_smem_raw + {lo_off} + boff) = lb;')
       else:
         self.w('const __nv_bfloat16 h = __float2bfloat16_rn(v);')
         self.w('const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));')
         self.w(f'*reinterpret_cast<__nv_bfloat16*>(tfb_smem_raw + {hi_off} + boff) = h;')
         self.w(f'*reinterpret_cast<__nv_bfloat16*>(tfb_smem_raw + {lo_off} + boff) = l;')
       self.close()
-    if hdr:
-      self.w(f'for (int q = threadIdx.x; q < {len(hdr)}; q += blockDim.x) sHdr[q] = shdr_{b}[q];')
-      self.w(f'for (int q = threadIdx.x; q < {len(pairs)}; q += blockDim.x) sPair[q] = spair_{b}[q];')
     self.open('if (threadIdx.x == 0)')
     for ti in range(nterms):
-      self.w(f'tfb_tc::mbar_init(&bars[{ti}], {128 * H}u);')
-      self.w(f'tfb_tc::mbar_init(&bars[{nterms + ti}], 1u);')
-    self.w(f'tfb_tc::mbar_init(&bars[{2 * nterms}], 1u);')
-    self.w(f'tfb_tc::mbar_init(&bars[{2 * nterms + 1}], 1u);')
+      self.w(f'tfb_tc::mbar_init(&bars[{BAR_FULL + ti}], {NP}u);')
+      self.w(f'tfb_tc::mbar_init(&bars[{BAR_FREE + ti}], 1u);')
+    self.w(f'tfb_tc::mbar_init(&bars[{BAR_DFULL}], 1u);')
+    self.w(f'tfb_tc::mbar_init(&bars[{BAR_DFREE}], {NP}u);')
     self.w('asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");')
     self.close()
     self.open('if (warp == 0)')
@@ -339,70 +393,83 @@ class _TC:
     self.w('tfb_tc::fence_after();')
     self.w('const unsigned tmem = *tmem_slot;')
     self.w('bool ok = true;')
-    # ---- MMA issuer: warp 4, one thread
+    # ---- MMA issuer
     self.open(f'if (warp == {4 * H})')
     self.open('if (lane == 0)')
     self.w('unsigned it = 0;')
     self.open('for (size_t tile = blockIdx.x; tile < numTiles && ok; tile += gridDim.x, ++it)')
-    self.w(f'const unsigned dcol = (it & 1u) ? {d_base[1]}u : {d_base[0]}u;')
+    self.w(f'if (it > 0 && !tfb_tc::mbar_wait(&bars[{BAR_DFREE}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 13u); break; }}')
+    mma = 'mma_tf32' if prec == 'tf32x3' else 'mma_f16'
     for ti, t in enumerate(s.terms):
       kp = lay['kpad'][ti]
       ksteps = kp // lay['ks']
       hi_off, lo_off = b_off[ti]
       sbo = (kp // ke) * 128
       acols = lay['a_cols'][ti]
-      self.w(f'if (!tfb_tc::mbar_wait(&bars[{ti}], it & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, {10 + ti}u); break; }}')
+      cps = lay['ks'] * es // 4
+      self.w(f'if (!tfb_tc::mbar_wait(&bars[{BAR_FULL + ti}], it & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, {10 + ti}u); break; }}')
       self.w('tfb_tc::fence_after();')
       self.open(f'for (int ks = 0; ks < {ksteps}; ++ks)')
-      # A from TMEM: hi at slot_base, lo at slot_base + acols; per k step advance K elems -> cols
-      cols_per_step = lay['ks'] * es // 4
-      self.w(f'const unsigned a_hi = tmem + {slot_base[ti]}u + ks * {cols_per_step}u;')
+      self.w(f'const unsigned a_hi = tmem + {slot_base[ti]}u + ks * {cps}u;')
       self.w(f'const unsigned a_lo = a_hi + {acols}u;')
-      self.w(f'const unsigned b_hi_addr = tfb_tc::smem_u32(tfb_smem_raw + {hi_off}) + ks * 256u;')
-      self.w(f'const unsigned b_lo_addr = tfb_tc::smem_u32(tfb_smem_raw + {lo_off}) + ks * 256u;')
-      self.w(f'const uint64_t bh = tfb_tc::smem_desc(b_hi_addr, 128u, {sbo}u);')
-      self.w(f'const uint64_t bl = tfb_tc::smem_desc(b_lo_addr, 128u, {sbo}u);')
-      mma = 'mma_tf32' if prec == 'tf32x3' else 'mma_f16'
+      self.w(f'const uint64_t bh = tfb_tc::smem_desc(tfb_tc::smem_u32(tfb_smem_raw + {hi_off}) + ks * 256u, 128u, {sbo}u);')
+      self.w(f'const uint64_t bl = tfb_tc::smem_desc(tfb_tc::smem_u32(tfb_smem_raw + {lo_off}) + ks * 256u, 128u, {sbo}u);')
       first = '(ks > 0) ? 1u : 0u' if ti == 0 else '1u'
-      self.w(f'tfb_tc::{mma}(tmem + dcol, a_hi, bh, {idesc}u, {first});')
-      self.w(f'tfb_tc::{mma}(tmem + dcol, a_hi, bl, {idesc}u, 1u);')
-      self.w(f'tfb_tc::{mma}(tmem + dcol, a_lo, bh, {idesc}u, 1u);')
+      self.w(f'tfb_tc::{mma}(tmem + {d_main}u, a_hi, bh, {idesc}u, {first});')
+      self.w(f'tfb_tc::{mma}(tmem + {d_corr}u, a_hi, bl, {idesc}u, {first});')
+      self.w(f'tfb_tc::{mma}(tmem + {d_corr}u, a_lo, bh, {idesc}u, 1u);')
       self.close()
-      self.w(f'tfb_tc::mma_commit(&bars[{nterms + ti}]);')
-    self.w(f'tfb_tc::mma_commit(&bars[{2 * nterms} + (it & 1u)]);')
+      self.w(f'tfb_tc::mma_commit(&bars[{BAR_FREE + ti}]);')
+    self.w(f'tfb_tc::mma_commit(&bars[{BAR_DFULL}]);')
     self.close()
     self.close()
     self.close()
-    # ---- producers / epilogue: warps 0-3, lane = TMEM lane = flat column within the tile
+    # ---- producers
     self.open(f'else if (warp < {4 * H})')
+    self.w('const unsigned ptid = threadIdx.x;')
     self.w('const unsigned quad = warp & 3u, grp = warp >> 2;')
     self.w('const unsigned row = quad * 32u + lane;')
     self.w('const unsigned lane_addr = tmem + ((quad * 32u) << 16);')
+    self.w(f'const bool lane_col = row < {tcols}u;')
+    self.w(f'const unsigned le = row / {s.N}u, lj = row - le * {s.N}u;')
     self.w('unsigned it = 0;')
     self.w('size_t prev_tile = 0; bool have_prev = false;')
+    self.open('if (blockIdx.x < numTiles)')
+    self._prefetch('(size_t)blockIdx.x', 'stage0')
+    self.close()
+    self.w('tfb_tc::cp_async_commit();')
     self.open('for (size_t tile = blockIdx.x; ; tile += gridDim.x, ++it)')
-    self.w('const bool more = tile < numTiles && ok;')
+    self.w('// every producer takes the same branches around named barriers: a timeout anywhere')
+    self.w('// stops all producers at the next tile boundary (a barrier-wide OR), never mid-tile')
+    self.w(f'if (tfb_tc::any_sync(1, {NP}, !ok)) break;')
+    self.w('const bool more = tile < numTiles;')
+    self.w('float* const cur = (it & 1u) ? stage1 : stage0;')
+    self.w('float* const nxt = (it & 1u) ? stage0 : stage1;')
     self.open('if (more)')
-    self.w('const size_t c = tile * 128u + row;')
-    self.w('const bool valid = c < totalCols;')
-    self.w(f'const size_t e = valid ? c / {s.N}u : 0;')
-    self.w(f'const int j = valid ? (int)(c - e * {s.N}u) : 0;')
-    self.w('const bool active = valid && (flags == nullptr || flags[e] != 0u);')
+    self.w('const size_t ntile = tile + gridDim.x;')
+    self.open('if (ntile < numTiles)')
+    self._prefetch('ntile', 'nxt')
+    self.close()
+    self.w('tfb_tc::cp_async_commit();')
+    self.w('tfb_tc::cp_async_wait_one();')
+    self.w(f'tfb_tc::named_sync(1, {NP});')
+    self.w(f'const size_t e0 = tile * {te}u;')
+    self.w('const size_t el = e0 + le;')
+    self.w('const bool active = lane_col && el < numElements && (flags == nullptr || flags[el] != 0u);')
     for ti, t in enumerate(s.terms):
-      self._produce_term(ti, t, slot_base[ti], lim)
+      self._term(ti, t, slot_base[ti], stage_off, lim, NP)
     self.close()
     # epilogue of the previous tile
-    self.open('if (have_prev && ok)')
-    self.w(f'const unsigned pb = ((it - 1u) & 1u);')
-    self.w(f'if (!tfb_tc::mbar_wait(&bars[{2 * nterms} + pb], ((it - 1u) >> 1) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 20u); }}')
-    self.open('if (ok)')
+    self.open('if (have_prev)')
+    self.w(f'if (!tfb_tc::mbar_wait(&bars[{BAR_DFULL}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 20u); }}')
     self.w('tfb_tc::fence_after();')
-    self._epilogue(d_base)
-    self.close()
+    self._epilogue(d_main, d_corr, NP)
     self.close()
     self.w('if (!more) break;')
     self.w('prev_tile = tile; have_prev = true;')
     self.close()
+    self.w('tfb_tc::cp_async_wait_all();')
+    self.w('if (ptid == 0) tfb_tc::bulk_wait();')
     self.close()
     # ---- teardown
     self.w('tfb_tc::fence_before();')
@@ -423,57 +490,113 @@ class _TC:
     pre = ('  int sms = 0;\n'
            '  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);\n'
            '  if (sms > 0 && grid.x > (unsigned)sms) grid.x = (unsigned)sms;')
-    launch = {'kernel': kname, 'block': nthreads, 'elements_per_block': 1, 'smem': smem, 'args': args,
-              'grid': f'(numElements * {s.N}u + 127u) / 128u', 'pre': pre}
+    launch = {'kernel': kname, 'block': nthreads, 'elements_per_block': te, 'smem': smem, 'args': args,
+              'grid': f'(numElements + {te - 1}u) / {te}u', 'pre': pre}
     return kernel, launch, ''
 
+  # ------------------------------------------------------------------ staging
+  def _prefetch(self, tile_expr, buf):
+    """cp.async the tile's batched operands into `buf` (16-byte chunks when aligned)."""
+    te = self.sm['te']
+    staged = staged_operands(self.s)
+    NP = 128 * self.H
+    off = 0
+    for op, vals in staged:
+      vp = _pad(vals, 4)
+      self.open('')
+      self.w(f'const size_t pe0 = ({tile_expr}) * {te}u;')
+      if vals % 4 == 0:
+        self.open(f'for (unsigned q = ptid; q < {te * vals // 4}u; q += {NP}u)')
+        self.w(f'const unsigned ei = q / {vals // 4}u, c4 = q - ei * {vals // 4}u;')
+        self.w('const size_t ee = pe0 + ei;')
+        self.open('if (ee < numElements)')
+        self.w(f'const float* src = {self._elem_ptr(op, "ee")} + 4u * c4;')
+        self.w(f'float* dst = {buf} + {off} + ei * {vp}u + 4u * c4;')
+        self.w('if ((reinterpret_cast<uintptr_t>(src) & 15u) == 0u) tfb_tc::cp_async16(dst, src);')
+        self.w('else { tfb_tc::cp_async4(dst, src); tfb_tc::cp_async4(dst + 1, src + 1); '
+               'tfb_tc::cp_async4(dst + 2, src + 2); tfb_tc::cp_async4(dst + 3, src + 3); }')
+        self.close()
+        self.close()
+      else:
+        self.open(f'for (unsigned q = ptid; q < {te * vals}u; q += {NP}u)')
+        self.w(f'const unsigned ei = q / {vals}u, c = q - ei * {vals}u;')
+        self.w('const size_t ee = pe0 + ei;')
+        self.w(f'if (ee < numElements) tfb_tc::cp_async4({buf} + {off} + ei * {vp}u + c, {self._elem_ptr(op, "ee")} + c);')
+        self.close()
+      self.close()
+      off += te * vp
+
   # ------------------------------------------------------------------ producer
-  def _produce_term(self, ti, t, slot_col, lim):
+  def _term(self, ti, t, slot_col, stage_off, lim, NP):
     b, LC = self.base, self.LC
+    s = self.s
     lay = self.lay
     prec = self.prec
-    es = lay['es']
     kp = lay['kpad'][ti]
     acols = lay['a_cols'][ti]
-    nterms = len(self.s.terms)
-    self.w(f'// term {ti}: U_{ti} column j -> tensor memory slot {ti} (hi at +0, lo at +{acols})')
+    nterms = len(s.terms)
+    pitch = self.sm['pitch']
+    te = self.sm['te']
+    H = self.H
+    bvals = _pad(t.B.element_volume(), 4)
+    self.w(f'// term {ti}: U_{ti} -> tensor memory slot {ti} (hi at +0, lo at +{acols})')
     self.open('')
-    # wait until the MMAs of the previous tile have finished reading this slot
+    if t.R is not None:
+      # U phase: one thread per (element, row l) computes row l of U_t for every column j
+      rvals = _pad(t.R.storage_size(), 4)
+      self.open(f'for (unsigned q = ptid; q < {te * t.K}u; q += {NP}u)')
+      self.w(f'const unsigned ei = q / {t.K}u, l = q - ei * {t.K}u;')
+      self.w(f'const float* bq = cur + {stage_off[t.B.name]} + ei * {bvals}u + l;')
+      self.w(f'const float* rq = cur + {stage_off[t.R.name]} + ei * {rvals}u;')
+      P = t.P
+      for m in range(P):
+        self.w(f'const float q{m} = bq[{m * t.K}];')
+      look = t.R.sparse_lookup() if t.R.sparse else None
+      for j in range(s.N):
+        terms = []
+        for m in range(P):
+          pos = (look.get((m, j)) if look is not None else j * P + m)
+          if pos is not None:
+            terms.append((m, pos))
+        expr = '0.0f'
+        for m, pos in terms:
+          expr = f'fmaf(q{m}, rq[{pos}], {expr})'
+        self.w(f'ubuf[(ei * {s.N}u + {j}u) * {pitch}u + l] = {expr};')
+      self.close()
+      self.w(f'tfb_tc::named_sync(1, {NP});')
+    # lane phase: wait for the slot, read the lane's column, split, store to TMEM
     self.w(f'if (it > 0 && !tfb_tc::mbar_wait(&bars[{nterms + ti}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, {30 + ti}u); }}')
     self.w('tfb_tc::fence_after();')
-    self._base(t.B, 'pB')
-    ms = 0
     if t.R is not None:
-      sl = r_slots(t)
-      ms = max(len(c) for c in sl)
-      self._base(t.R, 'pR')
-      self.w(f'const int2 hdr = active ? sHdr[{self._slot_hdr(ti)} + j] : make_int2(0, 0);')
-      for q in range(ms):
-        self.w(f'const int2 pr{q} = sPair[hdr.x + ({q} < hdr.y ? {q} : 0)];')
-        self.w(f'const float* const col{q} = ({q} < hdr.y) ? pB + pr{q}.x : zeros_{b};')
-        self.w(f'const float r{q} = ({q} < hdr.y) ? __ldg(pR + pr{q}.y) : 0.0f;')
+      src = f'(ubuf + row * {pitch}u)'
+      vec = True
+    else:
+      src = f'(cur + {stage_off[t.B.name]} + le * {bvals}u + lj * {t.K}u)'
+      vec = t.K % 4 == 0
     for ci, l0 in enumerate(range(0, kp, LC)):
       n = min(LC, kp - l0)
       real = max(0, min(n, t.K - l0))
-      self.open(f'if (grp == {ci % self.H}u)')
+      self.open(f'if (grp == {ci % H}u)')
       self.w(f'float u[{n}];')
       self.w('#pragma unroll')
       self.w(f'for (int i = 0; i < {n}; ++i) u[i] = 0.0f;')
       if real > 0:
-        if t.R is None:
-          self.open('if (active)')
-          self.w('#pragma unroll')
-          self.w(f'for (int i = 0; i < {real}; ++i) u[i] = __ldg(pB + (size_t)j * {t.K} + {l0} + i);')
-          self.close()
+        self.open('if (active)')
+        self.w(f'const float* p = {src} + {l0};')
+        if vec and l0 % 4 == 0:
+          for v in range(real // 4):
+            self.w(f'{{ const float4 x = *reinterpret_cast<const float4*>(p + {4 * v}); '
+                   f'u[{4*v}] = x.x; u[{4*v+1}] = x.y; u[{4*v+2}] = x.z; u[{4*v+3}] = x.w; }}')
+          for i in range(real // 4 * 4, real):
+            self.w(f'u[{i}] = p[{i}];')
         else:
-          for q in range(ms):
-            self.w('#pragma unroll')
-            self.w(f'for (int i = 0; i < {real}; ++i) u[i] = fmaf(r{q}, __ldg(col{q} + ({q} < hdr.y ? {l0} + i : i)), u[i]);')
-      # split and store hi/lo into TMEM (lane = row)
+          self.w('#pragma unroll')
+          self.w(f'for (int i = 0; i < {real}; ++i) u[i] = p[i];')
+        self.close()
       if prec == 'tf32x3':
         self.w(f'unsigned hv[{n}], lv[{n}];')
         self.w('#pragma unroll')
-        self.w(f'for (int i = 0; i < {n}; ++i) {{ hv[i] = tfb_tc::tf32_hi_bits(u[i]); lv[i] = __float_as_uint(u[i] - __uint_as_float(hv[i])); }}')
+        self.w(f'for (int i = 0; i < {n}; ++i) tfb_tc::tf32_split(u[i], hv[i], lv[i]);')
         for c8 in range(0, n, 8):
           self.w(f'tfb_tc::st_x8(lane_addr + {slot_col + l0 + c8}u, hv + {c8});')
           self.w(f'tfb_tc::st_x8(lane_addr + {slot_col + acols + l0 + c8}u, lv + {c8});')
@@ -495,52 +618,69 @@ class _TC:
     self.w('tfb_tc::st_wait();')
     self.w('tfb_tc::fence_before();')
     self.w(f'tfb_tc::mbar_arrive(&bars[{ti}]);')
+    # the transposition buffer (and, after the last term, the stage buffer) are reused next
+    self.w(f'tfb_tc::named_sync(1, {NP});')
     self.close()
 
-  def _slot_hdr(self, ti):
-    off = 0
-    for k, t in enumerate(self.s.terms):
-      if k == ti:
-        return off
-      if t.R is not None:
-        off += self.s.N
-    return off
-
-  def _epilogue(self, d_base):
+  def _epilogue(self, d_main, d_corr, NP):
     s = self.s
     M = s.M
-    nld = (M + 7) // 8
     H = self.H
-    self.w(f'const unsigned dcol = pb ? {d_base[1]}u : {d_base[0]}u;')
+    te = self.sm['te']
+    nld = (M + 7) // 8
     per = (nld + H - 1) // H
-    self.w(f'unsigned dv[{per * 8}];')
+    out = s.out
+    self.w(f'unsigned dv[{per * 8}], dc[{per * 8}];')
     for k in range(per):
-      # group g loads x8 block q = g + k*H (clamped; the duplicate is not stored)
-      self.w(f'tfb_tc::ld_x8(lane_addr + dcol + 8u * (grp + {k * H}u < {nld}u ? grp + {k * H}u : 0u), dv + {8 * k});')
+      blk = f'8u * (grp + {k * H}u < {nld}u ? grp + {k * H}u : 0u)'
+      self.w(f'tfb_tc::ld_x8(lane_addr + {d_main}u + {blk}, dv + {8 * k});')
+      self.w(f'tfb_tc::ld_x8(lane_addr + {d_corr}u + {blk}, dc + {8 * k});')
     self.w('tfb_tc::ld_wait();')
-    self.w('const size_t c = prev_tile * 128u + row;')
-    self.open('if (c < totalCols)')
-    self.w(f'const size_t e = c / {s.N}u;')
-    self.w(f'const int j = (int)(c - e * {s.N}u);')
-    self.open('if (flags == nullptr || flags[e] != 0u)')
-    self._base(s.out, 'pO')
-    self.w(f'float* const col = pO + (size_t)j * {M};')
+    self.w('tfb_tc::fence_before();')
+    self.w(f'tfb_tc::mbar_arrive(&bars[{2 * len(s.terms) + 1}]);')
+    self.w('#pragma unroll')
+    self.w(f'for (int i = 0; i < {per * 8}; ++i) dv[i] = __float_as_uint(__uint_as_float(dv[i]) + __uint_as_float(dc[i]));')
+    self.w(f'const size_t pe0 = prev_tile * {te}u;')
+    self.w('const size_t pel = pe0 + le;')
+    self.w('const bool pvalid = lane_col && pel < numElements;')
+    bulk_ok = (out.addressing.name == 'STRIDED' and not s.accumulate
+               and out.element_volume() == M * s.N and out.element_volume() % 4 == 0)
+    last = M - 8 * (nld - 1)
+    if bulk_ok:
+      # stage the tile's output contiguously and write it with one bulk copy
+      self.w(f'float* const obase = {out.name} + pe0 * {out.element_volume()}u + {out.name}_extraOffset;')
+      self.w(f'const size_t nvalid = (numElements - pe0) < {te}u ? (numElements - pe0) : {te}u;')
+      self.w('const bool bulk = flags == nullptr && ((reinterpret_cast<uintptr_t>(obase) & 15u) == 0u);')
+      self.open('if (bulk)')
+      self.open('if (pvalid)')
+      for k in range(per):
+        self.w(f'const unsigned q{k} = grp + {k * H}u;')
+        self.open(f'if (q{k} < {nld}u)')
+        self.w(f'float* const dst = ubuf + row * {M}u + 8u * q{k};')
+        self.w(f'const unsigned cnt = (q{k} == {nld - 1}u) ? {last}u : 8u;')
+        self.w(f'for (unsigned i = 0; i < cnt; ++i) dst[i] = __uint_as_float(dv[{8 * k} + i]);')
+        self.close()
+      self.close()
+      self.w('tfb_tc::fence_proxy_async();')
+      self.w(f'tfb_tc::named_sync(1, {NP});')
+      self.open('if (ptid == 0)')
+      self.w(f'tfb_tc::bulk_store(obase, ubuf, (unsigned)(nvalid * {out.element_volume() * 4}u));')
+      self.w('tfb_tc::bulk_wait_read();')
+      self.close()
+      self.w(f'tfb_tc::named_sync(1, {NP});')
+      self.close()
+      self.open('else if (pvalid && (flags == nullptr || flags[pel] != 0u))')
+    else:
+      self.open('if (pvalid && (flags == nullptr || flags[pel] != 0u))')
+    self.w(f'float* const col = {self._elem_ptr(out, "pel")} + (size_t)lj * {M}u;')
     for k in range(per):
       self.w(f'const unsigned q{k} = grp + {k * H}u;')
       self.open(f'if (q{k} < {nld}u)')
       self.w(f'float* const dst = col + 8u * q{k};')
-      last = M - 8 * (nld - 1)
       self.w(f'const unsigned cnt = (q{k} == {nld - 1}u) ? {last}u : 8u;')
       if s.accumulate:
         self.w(f'for (unsigned i = 0; i < cnt; ++i) dst[i] += __uint_as_float(dv[{8 * k} + i]);')
       else:
-        self.open('if (cnt == 8u && (reinterpret_cast<uintptr_t>(dst) & 15u) == 0u)')
-        self.w(f'reinterpret_cast<float4*>(dst)[0] = make_float4(__uint_as_float(dv[{8*k}]), __uint_as_float(dv[{8*k+1}]), __uint_as_float(dv[{8*k+2}]), __uint_as_float(dv[{8*k+3}]));')
-        self.w(f'reinterpret_cast<float4*>(dst)[1] = make_float4(__uint_as_float(dv[{8*k+4}]), __uint_as_float(dv[{8*k+5}]), __uint_as_float(dv[{8*k+6}]), __uint_as_float(dv[{8*k+7}]));')
-        self.close()
-        self.open('else')
         self.w(f'for (unsigned i = 0; i < cnt; ++i) dst[i] = __uint_as_float(dv[{8 * k} + i]);')
-        self.close()
       self.close()
-    self.close()
     self.close()
