@@ -314,11 +314,12 @@ def impl_ours(args, rank, world, dist):
   pk, pk_src = peaks()
   achieved = alg_bytes / (mean_launch / 1e3) / 1e9
   traffic = None
-  prof = os.path.join(ROOT, 'profiles', f'traffic_{pr["kernel"]}.json')
+  prof = os.path.join(ROOT, 'profiles', 'traffic.json')
   if os.path.exists(prof):
     with open(prof) as f:
-      tr = json.load(f)
-    traffic = tr.get('bytes_per_element', 0) * n + shared_bytes if 'bytes_per_element' in tr else tr.get('traffic')
+      tr = json.load(f).get(pr['plan'])
+    if tr is not None:
+      traffic = tr['bytes_per_element'] * n
   roofline = {'bound': 'hbm', 'achieved': achieved, 'peak': pk['hbm_gbs'], 'unit': 'GB/s',
               'frac': achieved / pk['hbm_gbs'], 'traffic': traffic,
               'peak_source': f'{pk_src} HBM copy bandwidth', 'kernel': pr['kernel'],

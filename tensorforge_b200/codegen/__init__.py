@@ -18,6 +18,7 @@ PRELUDE = '''#include <cuda_runtime.h>
 #include <cstdint>
 #include <cstddef>
 #include <atomic>
+#include <mutex>
 #include "tensorforge_aux.h"
 '''
 

@@ -146,25 +146,28 @@ def r_slots(term):
 
 
 def colprog_plan(chain, shape: LeftChain, fp_size, variant):
+  from ..codegen.colprog import tile_elements
   threads = variant.get('threads', 128)
-  chunk = variant.get('chunk')
-  kmax = max(t.K for t in shape.terms)
-  if chunk is None:
-    chunk = kmax if kmax <= 16 else 16
-  chunk = max(4, (chunk + 3) // 4 * 4)
+  chunk = variant.get('chunk', 16)
+  a_source = variant.get('a_source', 'const')
   vec = 4 if fp_size == 4 else 2
-  a_vals = 0
-  for t in shape.terms:
-    n = sum(len(rows) for _, rows in a_values(t))
-    a_vals += (n + vec - 1) // vec * vec
-  slot_entries = sum(sum(len(c) for c in r_slots(t)) for t in shape.terms if t.R is not None)
-  smem = a_vals * fp_size + 8 * (slot_entries + shape.N * len(shape.terms) + 4)
+  chunk = max(vec, (chunk + vec - 1) // vec * vec)
+  if shape.M > 128 or shape.N > threads:
+    return None
+  te = tile_elements(shape, threads)
+  kmax = max(t.K for t in shape.terms)
+  pitch = (kmax + vec - 1) // vec * vec + vec
+  a_vals = sum(t.A.storage_size() for t in shape.terms)
+  if a_source == 'const' and a_vals * fp_size > 48 * 1024:
+    a_source = 'smem'
+  smem = max(te * shape.N * pitch, te * shape.N * shape.M) * fp_size
+  if a_source == 'smem':
+    smem += (a_vals + vec) * fp_size
   if smem > SMEM_LIMIT:
     return None
-  if shape.M > 128:
-    return None
-  return Plan('colprog', {'threads': threads, 'chunk': chunk, 'min_blocks': variant.get('min_blocks', 0)},
-              smem, threads, note=f'M={shape.M} N={shape.N} terms={len(shape.terms)}')
+  return Plan('colprog', {'threads': threads, 'chunk': chunk, 'min_blocks': variant.get('min_blocks', 0),
+                          'a_source': a_source},
+              smem, threads, note=f'M={shape.M} N={shape.N} terms={len(shape.terms)} tile={te}')
 
 
 def tcsplit_plan(chain, shape, precision, variant):
