@@ -111,7 +111,14 @@ class _ColProg:
     self.a_total = total
     ubuf_vals = max(self.TC * self.pitch, self.TC * s.M)
     a_smem = _pad(self.a_total, self.VEC) if self.asrc == 'smem' else 0
-    self.smem = (ubuf_vals + a_smem) * self.FS
+    # per-tile copies of the batched R operands (read as 128-bit broadcast loads)
+    self.r_off = {}
+    r_vals = 0
+    for t in s.terms:
+      if t.R is not None and t.R.kind == 'batched' and t.R.name not in self.r_off:
+        self.r_off[t.R.name] = ubuf_vals + a_smem + r_vals
+        r_vals += self.TE * _pad(t.R.storage_size(), self.VEC)
+    self.smem = (ubuf_vals + a_smem + r_vals) * self.FS
     self.w(f'// generated by tensorforge_b200 (strategy: colprog, threads={BT}, chunk={self.LC}, '
            f'tile={self.TE} elements, A from {self.asrc})')
     self.w('// meta data:')
@@ -139,6 +146,17 @@ class _ColProg:
     self.w('const size_t el = e0 + le;')
     self.w(f'const bool lane_ok = threadIdx.x < {self.TC}u && el < numElements;')
     self.w('const bool active = lane_ok && (flags == nullptr || flags[el] != 0u);')
+    for name, off in self.r_off.items():
+      op = [o for o in self.chain.operands if o.name == name][0]
+      nr = op.storage_size()
+      nrp = _pad(nr, self.VEC)
+      self.open(f'for (unsigned q = threadIdx.x; q < {self.TE * nr}u; q += {BT}u)')
+      self.w(f'const unsigned ei = q / {nr}u, p = q - ei * {nr}u;')
+      self.w('const size_t e = e0 + ei;')
+      self.w(f'ubuf[{off} + ei * {nrp}u + p] = e < numElements ? __ldg({self._elem_ptr(op, "e")} + p) : {self.lit(0)};')
+      self.close()
+    if self.r_off:
+      self.w('__syncthreads();')
     self.w(f'{T} acc[{s.M}];')
     self.w('#pragma unroll')
     self.w(f'for (int i = 0; i < {s.M}; ++i) acc[i] = {self.lit(0)};')
@@ -206,31 +224,47 @@ class _ColProg:
     pitch = self.pitch
     self.w(f'// term {ti}: A={t.A.name} ({t.A.shape[0]}x{t.A.shape[1]}, {"sparse" if t.A.sparse else "dense"}), '
            f'B={t.B.name}, R={t.R.name if t.R is not None else "-"}')
-    # U phase
-    self.open(f'for (unsigned q = threadIdx.x; q < {self.TE * K}u; q += {BT}u)')
-    self.w(f'const unsigned ei = q / {K}u, l = q - ei * {K}u;')
+    # U phase: thread (group g, row l) with l = tid % KP2 computes row l of U_t for the
+    # elements g, g + groups, ... (compile-time trip count, loads of all elements in flight)
+    kp2 = 1
+    while kp2 < K:
+      kp2 *= 2
+    groups = max(1, BT // kp2)
+    per = (self.TE + groups - 1) // groups
+    self.open('')
+    self.w(f'const unsigned l = threadIdx.x & {kp2 - 1}u, g = threadIdx.x / {kp2}u;')
+    self.w('#pragma unroll')
+    self.open(f'for (unsigned k = 0; k < {per}u; ++k)')
+    self.w(f'const unsigned ei = g + k * {groups}u;')
     self.w('const size_t e = e0 + ei;')
+    self.open(f'if (l < {K}u && ei < {self.TE}u && e < numElements)')
     self.w(f'{T}* const urow = ubuf + ei * {s.N * pitch}u + l;')
-    self.open('if (e < numElements)')
     self.w(f'const {T}* const bq = {self._elem_ptr(t.B, "e")} + l;')
     if t.R is None:
       for j in range(s.N):
         self.w(f'urow[{j * pitch}] = __ldg(bq + {j * K});')
     else:
-      if t.R.kind == 'batched':
-        self.w(f'const {T}* const rq = {self._elem_ptr(t.R, "e")};')
-      else:
-        self.w(f'const {T}* const rq = {t.R.name};')
       for m in range(P):
         self.w(f'const {T} q{m} = __ldg(bq + {m * K});')
+      nr = t.R.storage_size()
+      comps = ['x', 'y', 'z', 'w'][:VEC]
+      if t.R.kind == 'batched':
+        nrp = _pad(nr, VEC)
+        self.w(f'const {VT}* const rq = reinterpret_cast<const {VT}*>(ubuf + {self.r_off[t.R.name]} + ei * {nrp}u);')
+        for v in range((nr + VEC - 1) // VEC):
+          self.w(f'const {VT} r{v} = rq[{v}];')
+        rv = lambda pos: f'r{pos // VEC}.{comps[pos % VEC]}'
+      else:
+        rv = lambda pos: f'__ldg({t.R.name} + {pos})'
       look = t.R.sparse_lookup() if t.R.sparse else None
       for j in range(s.N):
         expr = self.lit(0)
         for m in range(P):
           pos = look.get((m, j)) if look is not None else j * P + m
           if pos is not None:
-            expr = f'{FMA}(q{m}, __ldg(rq + {pos}), {expr})'
+            expr = f'{FMA}(q{m}, {rv(pos)}, {expr})'
         self.w(f'urow[{j * pitch}] = {expr};')
+    self.close()
     self.close()
     self.close()
     self.w('__syncthreads();')

@@ -87,10 +87,12 @@ def smem_plan(shape, precision):
   b_bytes = lay['b_bytes']
   off_stage = _pad(b_bytes, 128)
   off_u = off_stage + 2 * _pad(stage, 128)
-  off_bar = off_u + _pad(ubuf, 128)
+  # two transposition buffers (term t uses buffer t % 2) when they fit: saves a barrier per term
+  nbuf = 2 if off_u + 2 * _pad(ubuf, 128) + 256 <= 227 * 1024 else 1
+  off_bar = off_u + nbuf * _pad(ubuf, 128)
   total = off_bar + 256
-  return dict(off_stage=off_stage, stage=_pad(stage, 128), off_u=off_u, pitch=pitch,
-              off_bar=off_bar, total=total, te=te, tc=tc)
+  return dict(off_stage=off_stage, stage=_pad(stage, 128), off_u=off_u, pitch=pitch, nbuf=nbuf,
+              ubuf_bytes=_pad(ubuf, 128), off_bar=off_bar, total=total, te=te, tc=tc)
 
 
 def plan(chain, shape, precision, variant):
@@ -352,7 +354,8 @@ class _TC:
     self.w(f'unsigned* const tmem_slot = reinterpret_cast<unsigned*>(bars + {2 * nterms + 2});')
     self.w(f'float* const stage0 = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_stage"]});')
     self.w(f'float* const stage1 = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_stage"] + sm["stage"]});')
-    self.w(f'float* const ubuf = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_u"]});')
+    self.w(f'float* const ubuf0 = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_u"]});')
+    self.w(f'float* const ubuf1 = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_u"] + (sm["ubuf_bytes"] if sm["nbuf"] == 2 else 0)});')
     self.w('const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;')
     self.w(f'const size_t numTiles = (numElements + {te - 1}u) / {te}u;')
     # ---- setup: B operand, barriers, TMEM
@@ -541,34 +544,43 @@ class _TC:
     bvals = _pad(t.B.element_volume(), 4)
     self.w(f'// term {ti}: U_{ti} -> tensor memory slot {ti} (hi at +0, lo at +{acols})')
     self.open('')
+    ubuf = f'ubuf{ti % self.sm["nbuf"]}' if self.sm['nbuf'] == 2 else 'ubuf0'
     if t.R is not None:
-      # U phase: one thread per (element, row l) computes row l of U_t for every column j
+      # U phase: thread (element group g = ptid / KP2, row l = ptid % KP2) computes row l of
+      # U_t for every column j of elements g, g + NP/KP2, ... (no integer division)
       rvals = _pad(t.R.storage_size(), 4)
-      self.open(f'for (unsigned q = ptid; q < {te * t.K}u; q += {NP}u)')
-      self.w(f'const unsigned ei = q / {t.K}u, l = q - ei * {t.K}u;')
+      kp2 = 1
+      while kp2 < t.K:
+        kp2 *= 2
+      groups = max(1, NP // kp2)
+      self.w(f'const unsigned l = ptid & {kp2 - 1}u, g = ptid / {kp2}u;')
+      self.open(f'if (l < {t.K}u)')
+      self.open(f'for (unsigned ei = g; ei < {te}u; ei += {groups}u)')
       self.w(f'const float* bq = cur + {stage_off[t.B.name]} + ei * {bvals}u + l;')
-      self.w(f'const float* rq = cur + {stage_off[t.R.name]} + ei * {rvals}u;')
+      self.w(f'const float4* rq4 = reinterpret_cast<const float4*>(cur + {stage_off[t.R.name]} + ei * {rvals}u);')
       P = t.P
       for m in range(P):
         self.w(f'const float q{m} = bq[{m * t.K}];')
+      nr = t.R.storage_size()
+      for v in range((nr + 3) // 4):
+        self.w(f'const float4 r{v} = rq4[{v}];')
+      comp = ['x', 'y', 'z', 'w']
       look = t.R.sparse_lookup() if t.R.sparse else None
       for j in range(s.N):
-        terms = []
+        expr = '0.0f'
         for m in range(P):
           pos = (look.get((m, j)) if look is not None else j * P + m)
           if pos is not None:
-            terms.append((m, pos))
-        expr = '0.0f'
-        for m, pos in terms:
-          expr = f'fmaf(q{m}, rq[{pos}], {expr})'
-        self.w(f'ubuf[(ei * {s.N}u + {j}u) * {pitch}u + l] = {expr};')
+            expr = f'fmaf(q{m}, r{pos // 4}.{comp[pos % 4]}, {expr})'
+        self.w(f'{ubuf}[(ei * {s.N}u + {j}u) * {pitch}u + l] = {expr};')
+      self.close()
       self.close()
       self.w(f'tfb_tc::named_sync(1, {NP});')
     # lane phase: wait for the slot, read the lane's column, split, store to TMEM
     self.w(f'if (it > 0 && !tfb_tc::mbar_wait(&bars[{nterms + ti}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, {30 + ti}u); }}')
     self.w('tfb_tc::fence_after();')
     if t.R is not None:
-      src = f'(ubuf + row * {pitch}u)'
+      src = f'({ubuf} + row * {pitch}u)'
       vec = True
     else:
       src = f'(cur + {stage_off[t.B.name]} + le * {bvals}u + lj * {t.K}u)'
@@ -596,7 +608,7 @@ class _TC:
       if prec == 'tf32x3':
         self.w(f'unsigned hv[{n}], lv[{n}];')
         self.w('#pragma unroll')
-        self.w(f'for (int i = 0; i < {n}; ++i) tfb_tc::tf32_split(u[i], hv[i], lv[i]);')
+        self.w(f'for (int i = 0; i < {n}; ++i) {{ hv[i] = tfb_tc::tf32_rna(u[i]); lv[i] = __float_as_uint(u[i] - __uint_as_float(hv[i])); }}')
         for c8 in range(0, n, 8):
           self.w(f'tfb_tc::st_x8(lane_addr + {slot_col + l0 + c8}u, hv + {c8});')
           self.w(f'tfb_tc::st_x8(lane_addr + {slot_col + acols + l0 + c8}u, lv + {c8});')
@@ -618,8 +630,10 @@ class _TC:
     self.w('tfb_tc::st_wait();')
     self.w('tfb_tc::fence_before();')
     self.w(f'tfb_tc::mbar_arrive(&bars[{ti}]);')
-    # the transposition buffer (and, after the last term, the stage buffer) are reused next
-    self.w(f'tfb_tc::named_sync(1, {NP});')
+    # the transposition buffer of this term is reused two terms later (or next term with one
+    # buffer), and the stage / buffers are reused after the last term
+    if self.sm['nbuf'] == 1 or ti == len(s.terms) - 1:
+      self.w(f'tfb_tc::named_sync(1, {NP});')
     self.close()
 
   def _epilogue(self, d_main, d_corr, NP):
@@ -656,15 +670,19 @@ class _TC:
       for k in range(per):
         self.w(f'const unsigned q{k} = grp + {k * H}u;')
         self.open(f'if (q{k} < {nld}u)')
-        self.w(f'float* const dst = ubuf + row * {M}u + 8u * q{k};')
-        self.w(f'const unsigned cnt = (q{k} == {nld - 1}u) ? {last}u : 8u;')
-        self.w(f'for (unsigned i = 0; i < cnt; ++i) dst[i] = __uint_as_float(dv[{8 * k} + i]);')
+        self.w(f'float* const dst = ubuf0 + row * {M}u + 8u * q{k};')
+        if M % 8 == 0:
+          self.w(f'reinterpret_cast<float4*>(dst)[0] = make_float4(__uint_as_float(dv[{8*k}]), __uint_as_float(dv[{8*k+1}]), __uint_as_float(dv[{8*k+2}]), __uint_as_float(dv[{8*k+3}]));')
+          self.w(f'reinterpret_cast<float4*>(dst)[1] = make_float4(__uint_as_float(dv[{8*k+4}]), __uint_as_float(dv[{8*k+5}]), __uint_as_float(dv[{8*k+6}]), __uint_as_float(dv[{8*k+7}]));')
+        else:
+          self.w(f'const unsigned cnt = (q{k} == {nld - 1}u) ? {last}u : 8u;')
+          self.w(f'for (unsigned i = 0; i < cnt; ++i) dst[i] = __uint_as_float(dv[{8 * k} + i]);')
         self.close()
       self.close()
       self.w('tfb_tc::fence_proxy_async();')
       self.w(f'tfb_tc::named_sync(1, {NP});')
       self.open('if (ptid == 0)')
-      self.w(f'tfb_tc::bulk_store(obase, ubuf, (unsigned)(nvalid * {out.element_volume() * 4}u));')
+      self.w(f'tfb_tc::bulk_store(obase, ubuf0, (unsigned)(nvalid * {out.element_volume() * 4}u));')
       self.w('tfb_tc::bulk_wait_read();')
       self.close()
       self.w(f'tfb_tc::named_sync(1, {NP});')

@@ -147,7 +147,7 @@ def r_slots(term):
 
 def colprog_plan(chain, shape: LeftChain, fp_size, variant):
   from ..codegen.colprog import tile_elements
-  threads = variant.get('threads', 128)
+  threads = variant.get('threads', 256)
   chunk = variant.get('chunk', 16)
   a_source = variant.get('a_source', 'const')
   vec = 4 if fp_size == 4 else 2
@@ -161,6 +161,8 @@ def colprog_plan(chain, shape: LeftChain, fp_size, variant):
   if a_source == 'const' and a_vals * fp_size > 48 * 1024:
     a_source = 'smem'
   smem = max(te * shape.N * pitch, te * shape.N * shape.M) * fp_size
+  smem += sum(te * ((t.R.storage_size() + vec - 1) // vec * vec) for t in shape.terms
+              if t.R is not None and t.R.kind == 'batched') * fp_size
   if a_source == 'smem':
     smem += (a_vals + vec) * fp_size
   if smem > SMEM_LIMIT:
