@@ -224,6 +224,77 @@ def impl_reference(args, rank, world):
 
 # ----------------------------------------------------------------------------- ours
 
+def extra_workloads(stream, short=False):
+  """Secondary BASELINE configs measured next to the headline (device-resident inputs)."""
+  import torch
+  from oracle import cases
+  from tensorforge_b200.kernels import make
+  from tensorforge_b200.runtime import compile_generator
+  out = {}
+  dev = torch.device('cuda')
+  # config 0: C_e = A * B_e, 56x56 * 56x9, pointer arrays
+  for n in ((10000,) if short else (10000, 1000000)):
+    g = make('c0_gemm_ptr', 'float')
+    k = compile_generator(g)
+    sym = {t.name: t for t, _ in g.abi_symbols()}
+    kw = {'numElements': n}
+    keep = []
+    for name, t in sym.items():
+      if t.addressing.name == 'NONE':
+        kw[name] = torch.rand(t.get_real_volume(), device=dev)
+      else:
+        buf = torch.rand(n * 504, device=dev)
+        ptrs = buf.data_ptr() + torch.arange(n, device=dev, dtype=torch.int64) * 504 * 4
+        keep.append(buf)
+        kw[name] = ptrs
+    total, per = time_launches(lambda: k(**kw), stream, 10, 3)
+    ms = sum(per) / len(per)
+    flops = n * g.get_chain().nz_flops_per_element()
+    out[f'c0_gemm_{n}'] = {'elements_per_s': n / (ms / 1e3), 'gflops': flops / (ms / 1e3) / 1e9, 'ms': ms,
+                           'plan': g.get_plan().key()}
+  # config 3: mixed shapes, one persistent launch over a work table, replayed from a CUDA graph
+  from tensorforge_b200.kernels import grouped_catalogue
+  gk = dict(grouped_catalogue())['bench_c3']
+  groups = cases.mixed_shape_groups()
+  kws, total_el, nz = [], 0, 0.0
+  for g, (b, q, n) in zip(gk.gens, groups):
+    kw = {'numElements': n}
+    for t, _ in g.abi_symbols():
+      size = t.spp.count_nz() if t.addressing.name == 'NONE' else n * t.get_real_volume()
+      kw[t.name] = torch.rand(size, device=dev) * 2 - 1
+    kws.append(kw)
+    total_el += n
+    nz += n * g.get_chain().nz_flops_per_element()
+  launch = gk.prepare(kws)
+  launch.capture()
+  total, per = time_launches(launch.replay, stream, 10, 3)
+  ms = sum(per) / len(per)
+  sep = [compile_generator(g) for g in gk.gens]
+
+  def separate():
+    for k, kw in zip(sep, kws):
+      k(**kw)
+  total2, per2 = time_launches(separate, stream, 5, 2)
+  ms2 = sum(per2) / len(per2)
+  out['c3_mixed_shapes'] = {'elements': total_el, 'groups': len(groups), 'elements_per_s': total_el / (ms / 1e3),
+                            'nz_gflops': nz / (ms / 1e3) / 1e9, 'ms': ms, 'launch': 'one persistent kernel, CUDA graph replay',
+                            'separate_launches_ms': ms2, 'separate_elements_per_s': total_el / (ms2 / 1e3)}
+  # FP64 order-6 chain
+  n = 100000 if short else 500000
+  for label, opts in (('fp64_plain', {}),):
+    g = make(CASE, 'double', **opts)
+    k = compile_generator(g)
+    kw = {'numElements': n}
+    for t, _ in g.abi_symbols():
+      size = t.spp.count_nz() if t.addressing.name == 'NONE' else n * t.get_real_volume()
+      kw[t.name] = torch.rand(size, device=dev, dtype=torch.float64) * 2 - 1
+    total, per = time_launches(lambda: k(**kw), stream, 5, 2)
+    ms = sum(per) / len(per)
+    out[f'chain_o6_{label}'] = {'elements_per_s': n / (ms / 1e3), 'plan': g.get_plan().key(), 'elements': n,
+                                'nz_gflops': n * g.get_chain().nz_flops_per_element() / (ms / 1e3) / 1e9}
+  return out
+
+
 def impl_ours(args, rank, world, dist):
   import torch
   from oracle import cases
@@ -343,6 +414,7 @@ def impl_ours(args, rank, world, dist):
       'elements_per_s': n / (sum(r['launch_ms']) / len(r['launch_ms']) / 1e3), 'plan': r['plan'],
       'rel_l2': r['accuracy']['rel_l2'], 'max_abs': r['accuracy']['max_abs']}
   cpu = reference_cpu() if (world == 1 and not args.no_cpu) else None
+  extras = extra_workloads(stream, short=args.no_cpu) if (world == 1 and not args.no_extras) else None
   line = {
     'metric': METRIC, 'value': value, 'unit': 'elements/s', 'n_gpus': world, 'steps': args.steps,
     'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
@@ -359,6 +431,8 @@ def impl_ours(args, rank, world, dist):
     'clocks': clocks.summary(),
   }
   line.update(extra_out)
+  if extras is not None:
+    line['other_configs'] = extras
   print(json.dumps(line))
 
 
@@ -372,6 +446,7 @@ def main():
   ap.add_argument('--elements', type=int, default=500000)
   ap.add_argument('--ref-sample', type=int, default=4096)
   ap.add_argument('--no-cpu', action='store_true')
+  ap.add_argument('--no-extras', action='store_true')
   args = ap.parse_args()
   rank = int(os.environ.get('RANK', '0'))
   world = int(os.environ.get('WORLD_SIZE', '1'))

@@ -194,3 +194,27 @@ def build(name, ns):
 
 def num_elements(name):
   return CASES[name][2]
+
+
+MIXED_BASES = (10, 20, 35, 56, 84)
+MIXED_QUANTITIES = (9, 27)
+
+
+def mixed_shape_groups(total=1_500_000, seed=0, lo=1_000, hi=200_000):
+  """basis sizes {10,20,35,56,84} x quantity counts {9,27}.
+
+  Returns [(basis, quantities, element count)], counts drawn log-uniform over lo..hi from
+  `seed`, rescaled to sum to ~`total`, each rounded to a multiple of 8.
+  """
+  rng = np.random.default_rng(seed)
+  shapes = [(b, q) for b in MIXED_BASES for q in MIXED_QUANTITIES]
+  raw = np.exp(rng.uniform(np.log(lo), np.log(hi), len(shapes)))
+  raw = raw * (total / raw.sum())
+  counts = [max(8, int(round(c / 8)) * 8) for c in raw]
+  return [(b, q, c) for (b, q), c in zip(shapes, counts)]
+
+
+def mixed_chain(ns, basis, quantities, seed=0):
+  """The order-`basis` volume chain with patterns seeded per shape (S density ~30%)."""
+  nnz = max(1, int(round(0.3 * quantities * quantities)))
+  return volume_chain(ns, basis=basis, quantities=quantities, s_nnz=nnz, seed=seed * 100 + basis * 7 + quantities)

@@ -28,6 +28,26 @@ def _pad(x, m):
   return (x + m - 1) // m * m
 
 
+CP_HELPERS = r'''
+#ifndef TFB_CP_ASYNC_HELPERS
+#define TFB_CP_ASYNC_HELPERS
+namespace tfb_cp {
+__device__ __forceinline__ void copy16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void copy4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void copy8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" :: "r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+}  // namespace tfb_cp
+#endif
+'''
+
+
 def emit_colprog(chain, plan, context, base_name, globals_):
   shape = match_left_chain(chain)
   return _ColProg(chain, shape, plan, context, base_name).emit(globals_)
@@ -53,6 +73,7 @@ class _ColProg:
     self.BT = plan.params['threads']
     self.LC = plan.params['chunk']
     self.asrc = plan.params.get('a_source', 'const')
+    self.prefetch = bool(plan.params.get('prefetch', 1)) and not getattr(self, 'grouped', False)
     self.TE = tile_elements(shape, self.BT)
     self.TC = self.TE * shape.N
     self.kmax = max(t.K for t in shape.terms)
@@ -97,11 +118,8 @@ class _ColProg:
     return f'{op.name}'
 
   # ------------------------------------------------------------------ emit
-  def emit(self, globals_):
+  def _layout(self):
     s = self.s
-    T, BT, VT = self.T, self.BT, self.VT
-    b = self.base
-    kname = f'kernel_{b}'
     # A storage: every term's values, in storage order, concatenated
     self.a_base = []
     total = 0
@@ -109,23 +127,103 @@ class _ColProg:
       self.a_base.append(total)
       total += t.A.storage_size()
     self.a_total = total
-    ubuf_vals = max(self.TC * self.pitch, self.TC * s.M)
-    a_smem = _pad(self.a_total, self.VEC) if self.asrc == 'smem' else 0
+    self.ubuf_vals = max(self.TC * self.pitch, self.TC * s.M)
     # per-tile copies of the batched R operands (read as 128-bit broadcast loads)
     self.r_off = {}
     r_vals = 0
     for t in s.terms:
       if t.R is not None and t.R.kind == 'batched' and t.R.name not in self.r_off:
-        self.r_off[t.R.name] = ubuf_vals + a_smem + r_vals
+        self.r_off[t.R.name] = self.ubuf_vals + r_vals
         r_vals += self.TE * _pad(t.R.storage_size(), self.VEC)
-    self.smem = (ubuf_vals + a_smem + r_vals) * self.FS
-    self.w(f'// generated by tensorforge_b200 (strategy: colprog, threads={BT}, chunk={self.LC}, '
+    self.work_vals = _pad(self.ubuf_vals + r_vals, self.VEC)   # ubuf + staged R, per CTA
+    # prefetch stage: the next tile's batched B / R operands, copied with cp.async while the
+    # last K stage of the current tile runs (standalone kernels only)
+    self.stage_off, self.stage_vals = {}, 0
+    if self.prefetch:
+      for t in s.terms:
+        for op in (t.B, t.R):
+          if op is not None and op.kind == 'batched' and op.name not in self.stage_off:
+            self.stage_off[op.name] = self.work_vals + self.stage_vals
+            self.stage_vals += self.TE * _pad(op.storage_size() if op.sparse else op.element_volume(), self.VEC)
+    a_smem = _pad(self.a_total, self.VEC) if self.asrc == 'smem' else 0
+    self.a_off = self.work_vals + self.stage_vals
+    self.smem = (self.work_vals + self.stage_vals + a_smem) * self.FS
+
+  def _header(self):
+    if self.prefetch:
+      self.w(CP_HELPERS)
+    self.w(f'// generated by tensorforge_b200 (strategy: colprog, threads={self.BT}, chunk={self.LC}, '
            f'tile={self.TE} elements, A from {self.asrc})')
     self.w('// meta data:')
     for o in self.chain.operands:
       self.w(f'// {o.tensor.gen_descr()}')
     for st in self.chain.stages:
       self.w(f'// {st.descr}')
+
+  def _prefetch(self, tile_expr):
+    """cp.async the tile's batched B / R operands into the stage (16-byte chunks when aligned)."""
+    T, BT, VEC, FS = self.T, self.BT, self.VEC, self.FS
+    ops = {o.name: o for o in self.chain.operands}
+    for name, off in self.stage_off.items():
+      op = ops[name]
+      vals = op.storage_size() if op.sparse else op.element_volume()
+      vp = _pad(vals, VEC)
+      self.open('')
+      self.w(f'const size_t pe0 = ({tile_expr}) * {self.TE}u;')
+      if vals % VEC == 0:
+        self.open(f'for (unsigned q = threadIdx.x; q < {self.TE * vals // VEC}u; q += {BT}u)')
+        self.w(f'const unsigned ei = q / {vals // VEC}u, c = q - ei * {vals // VEC}u;')
+        self.w('const size_t ee = pe0 + ei;')
+        self.open('if (ee < numElements)')
+        self.w(f'const {T}* src = {self._elem_ptr(op, "ee")} + {VEC}u * c;')
+        self.w(f'{T}* dst = ubuf + {off} + ei * {vp}u + {VEC}u * c;')
+        small = 'copy8' if FS == 8 else 'copy4'
+        self.w('if ((reinterpret_cast<uintptr_t>(src) & 15u) == 0u) tfb_cp::copy16(dst, src);')
+        self.w('else { ' + ' '.join(f'tfb_cp::{small}(dst + {i}, src + {i});' for i in range(VEC)) + ' }')
+        self.close()
+        self.close()
+      else:
+        small = 'copy8' if FS == 8 else 'copy4'
+        self.open(f'for (unsigned q = threadIdx.x; q < {self.TE * vals}u; q += {BT}u)')
+        self.w(f'const unsigned ei = q / {vals}u, c = q - ei * {vals}u;')
+        self.w('const size_t ee = pe0 + ei;')
+        self.w(f'if (ee < numElements) tfb_cp::{small}(ubuf + {off} + ei * {vp}u + c, {self._elem_ptr(op, "ee")} + c);')
+        self.close()
+      self.close()
+
+  def _tile_body(self):
+    """Code for one tile; expects `tile`, `ubuf`, (`sA`), the ABI names, numElements, flags."""
+    s, T, BT = self.s, self.T, self.BT
+    self.w(f'const unsigned le = threadIdx.x / {s.N}u, lj = threadIdx.x - le * {s.N}u;')
+    self.w(f'const size_t e0 = tile * {self.TE}u;')
+    self.w('const size_t el = e0 + le;')
+    self.w(f'const bool lane_ok = threadIdx.x < {self.TC}u && el < numElements;')
+    self.w('const bool active = lane_ok && (flags == nullptr || flags[el] != 0u);')
+    for name, off in ([] if self.prefetch else self.r_off.items()):
+      op = [o for o in self.chain.operands if o.name == name][0]
+      nr = op.storage_size()
+      nrp = _pad(nr, self.VEC)
+      self.open(f'for (unsigned q = threadIdx.x; q < {self.TE * nr}u; q += {BT}u)')
+      self.w(f'const unsigned ei = q / {nr}u, p = q - ei * {nr}u;')
+      self.w('const size_t e = e0 + ei;')
+      self.w(f'ubuf[{off} + ei * {nrp}u + p] = e < numElements ? __ldg({self._elem_ptr(op, "e")} + p) : {self.lit(0)};')
+      self.close()
+    if self.r_off and not self.prefetch:
+      self.w('__syncthreads();')
+    self.w(f'{T} acc[{s.M}];')
+    self.w('#pragma unroll')
+    self.w(f'for (int i = 0; i < {s.M}; ++i) acc[i] = {self.lit(0)};')
+    for ti, t in enumerate(s.terms):
+      self._term(ti, t)
+    self._store()
+
+  def emit(self, globals_):
+    s = self.s
+    T, BT = self.T, self.BT
+    b = self.base
+    kname = f'kernel_{b}'
+    self._layout()
+    self._header()
     if self.asrc == 'const':
       self.w(f'__constant__ {T} cA_{b}[{self.a_total}];')
     mb = self.plan.params.get('min_blocks', 0)
@@ -135,39 +233,68 @@ class _ColProg:
     self.w('extern __shared__ __align__(16) unsigned char tfb_smem_raw[];')
     self.w(f'{T}* const ubuf = reinterpret_cast<{T}*>(tfb_smem_raw);')
     if self.asrc == 'smem':
-      self.w(f'{T}* const sA = ubuf + {ubuf_vals};')
+      self.w(f'{T}* const sA = ubuf + {self.a_off};')
       for ti, t in enumerate(s.terms):
         self.w(f'for (int q = threadIdx.x; q < {t.A.storage_size()}; q += {BT}) sA[{self.a_base[ti]} + q] = {t.A.name}[q];')
       self.w('__syncthreads();')
     self.w(f'const size_t numTiles = (numElements + {self.TE - 1}u) / {self.TE}u;')
-    self.w(f'const unsigned le = threadIdx.x / {s.N}u, lj = threadIdx.x - le * {s.N}u;')
+    if self.prefetch:
+      self.w('if (blockIdx.x < numTiles) {')
+      self.ind += 1
+      self._prefetch('(size_t)blockIdx.x')
+      self.ind -= 1
+      self.w('}')
+      self.w('tfb_cp::commit();')
     self.open('for (size_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x)')
-    self.w(f'const size_t e0 = tile * {self.TE}u;')
-    self.w('const size_t el = e0 + le;')
-    self.w(f'const bool lane_ok = threadIdx.x < {self.TC}u && el < numElements;')
-    self.w('const bool active = lane_ok && (flags == nullptr || flags[el] != 0u);')
-    for name, off in self.r_off.items():
-      op = [o for o in self.chain.operands if o.name == name][0]
-      nr = op.storage_size()
-      nrp = _pad(nr, self.VEC)
-      self.open(f'for (unsigned q = threadIdx.x; q < {self.TE * nr}u; q += {BT}u)')
-      self.w(f'const unsigned ei = q / {nr}u, p = q - ei * {nr}u;')
-      self.w('const size_t e = e0 + ei;')
-      self.w(f'ubuf[{off} + ei * {nrp}u + p] = e < numElements ? __ldg({self._elem_ptr(op, "e")} + p) : {self.lit(0)};')
-      self.close()
-    if self.r_off:
+    if self.prefetch:
+      self.w('tfb_cp::wait_all();')
       self.w('__syncthreads();')
-    self.w(f'{T} acc[{s.M}];')
-    self.w('#pragma unroll')
-    self.w(f'for (int i = 0; i < {s.M}; ++i) acc[i] = {self.lit(0)};')
-    for ti, t in enumerate(s.terms):
-      self._term(ti, t)
-    self._store()
+    self._tile_body()
     self.close()
+    if self.prefetch:
+      self.w('tfb_cp::wait_all();')
     self.ind -= 1
     self.w('}')
     kernel = '\n'.join(self.lines)
     return kernel, self._launch(globals_, kname), ''
+
+  # ------------------------------------------------------------------ grouped launches
+  def emit_group_functions(self, globals_, gid):
+    """Device functions for one group of a grouped (mixed-shape) launch: A staging and one tile.
+
+    The group's ABI symbols arrive through a tfb_group_args record (pointers, extra offsets,
+    element count, flags); A is read from shared memory (staged when the group changes).
+    """
+    assert self.asrc == 'smem'
+    s, T, BT = self.s, self.T, self.BT
+    self._layout()
+    self._header()
+    decl = []
+    for i, (t, _) in enumerate(globals_):
+      dt = self.T if t.datatype is None else str(t.datatype)
+      const = 'const ' if t.direction.name == 'SOURCE' else ''
+      ptr = t.addressing.to_pointer()
+      decl.append(f'{const}{dt}{ptr} const __restrict__ {t.name} = reinterpret_cast<{const}{dt}{ptr}>(const_cast<void*>(ga.ptr[{i}]));')
+      if t.addressing.name != 'NONE':
+        decl.append(f'const unsigned {t.name}_extraOffset = ga.off[{i}];')
+    self.w(f'__device__ __forceinline__ void group{gid}_stage_a(const tfb_group_args& ga, {T}* sA) {{')
+    self.ind += 1
+    for d in decl:
+      self.w(d)
+    for ti, t in enumerate(s.terms):
+      self.w(f'for (int q = threadIdx.x; q < {t.A.storage_size()}; q += {BT}) sA[{self.a_base[ti]} + q] = {t.A.name}[q];')
+    self.ind -= 1
+    self.w('}')
+    self.w(f'__device__ __forceinline__ void group{gid}_tile(const tfb_group_args& ga, size_t tile, {T}* ubuf, const {T}* sA) {{')
+    self.ind += 1
+    for d in decl:
+      self.w(d)
+    self.w('const size_t numElements = (size_t)ga.num_elements;')
+    self.w('const unsigned* const flags = ga.flags;')
+    self._tile_body()
+    self.ind -= 1
+    self.w('}')
+    return '\n'.join(self.lines)
 
   def _launch(self, globals_, kname):
     s, BT, b = self.s, self.BT, self.base
@@ -239,18 +366,25 @@ class _ColProg:
     self.w('const size_t e = e0 + ei;')
     self.open(f'if (l < {K}u && ei < {self.TE}u && e < numElements)')
     self.w(f'{T}* const urow = ubuf + ei * {s.N * pitch}u + l;')
-    self.w(f'const {T}* const bq = {self._elem_ptr(t.B, "e")} + l;')
+    if self.prefetch:
+      bv = _pad(t.B.element_volume(), VEC)
+      self.w(f'const {T}* const bq = ubuf + {self.stage_off[t.B.name]} + ei * {bv}u + l;')
+      ld = lambda x: f'bq[{x}]'
+    else:
+      self.w(f'const {T}* const bq = {self._elem_ptr(t.B, "e")} + l;')
+      ld = lambda x: f'__ldg(bq + {x})'
     if t.R is None:
       for j in range(s.N):
-        self.w(f'urow[{j * pitch}] = __ldg(bq + {j * K});')
+        self.w(f'urow[{j * pitch}] = {ld(j * K)};')
     else:
       for m in range(P):
-        self.w(f'const {T} q{m} = __ldg(bq + {m * K});')
+        self.w(f'const {T} q{m} = {ld(m * K)};')
       nr = t.R.storage_size()
       comps = ['x', 'y', 'z', 'w'][:VEC]
       if t.R.kind == 'batched':
         nrp = _pad(nr, VEC)
-        self.w(f'const {VT}* const rq = reinterpret_cast<const {VT}*>(ubuf + {self.r_off[t.R.name]} + ei * {nrp}u);')
+        roff = self.stage_off[t.R.name] if self.prefetch else self.r_off[t.R.name]
+        self.w(f'const {VT}* const rq = reinterpret_cast<const {VT}*>(ubuf + {roff} + ei * {nrp}u);')
         for v in range((nr + VEC - 1) // VEC):
           self.w(f'const {VT} r{v} = rq[{v}];')
         rv = lambda pos: f'r{pos // VEC}.{comps[pos % VEC]}'
@@ -268,6 +402,12 @@ class _ColProg:
     self.close()
     self.close()
     self.w('__syncthreads();')
+    if self.prefetch and ti == len(s.terms) - 1:
+      self.w('// the stage is free: fetch the next tile while this K stage runs')
+      self.open('if (tile + gridDim.x < numTiles)')
+      self._prefetch('tile + gridDim.x')
+      self.close()
+      self.w('tfb_cp::commit();')
     # K stage
     self.open('if (active)')
     self.w(f'const {T}* const ucol = ubuf + threadIdx.x * {pitch}u;')

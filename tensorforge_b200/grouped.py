@@ -1,0 +1,244 @@
+"""Mixed-shape batched launches: one persistent kernel over a device work table.
+
+A `GroupedKernel` fuses several generated chains of the shared-left form (plan/chains.py),
+typically the same operation at different basis sizes and quantity counts, into one
+persistent kernel:
+
+  * each group contributes a tile function (codegen/colprog.py, CUDA cores, A staged in
+    shared memory) specialised at generation time for its shape and sparsity patterns;
+  * a device work table lists (group, tile) items ordered by group; CTAs (SMs x
+    occupancy) pull items with one atomic counter and run the matching tile function,
+    restaging the group's A values only when their group changes;
+  * the counter is reset on the launch stream, so launch + reset can be captured in a CUDA
+    graph and replayed (`capture()`).
+
+C ABI of the emitted library (one per fused set):
+
+    int tfb_grouped_launch_<name>(const tfb_group_args* args, const uint2* items,
+                                  unsigned num_items, unsigned* counter, void* stream);
+
+`args[g]` holds group g's ABI symbols in its launcher order (pointer or pointer array,
+extra offset), its element count and flags; `items` are (group, tile) pairs; `counter` is
+one device word of scratch that the launcher zeroes before the kernel.
+"""
+import ctypes
+import hashlib
+
+from .common.basic_types import Addressing
+from .common.exceptions import GenerationError
+from .plan import Plan
+from .plan.chains import match_left_chain
+from .codegen.colprog import _ColProg, _pad
+from .runtime.build import build_library
+
+MAX_SYMBOLS = 16
+
+ARGS_STRUCT = f'''
+#ifndef TFB_GROUP_ARGS
+#define TFB_GROUP_ARGS
+struct tfb_group_args {{
+  const void* ptr[{MAX_SYMBOLS}];
+  unsigned off[{MAX_SYMBOLS}];
+  unsigned long long num_elements;
+  const unsigned* flags;
+}};
+#endif
+'''
+
+
+class _GroupArgs(ctypes.Structure):
+  _fields_ = [('ptr', ctypes.c_void_p * MAX_SYMBOLS), ('off', ctypes.c_uint * MAX_SYMBOLS),
+              ('num_elements', ctypes.c_ulonglong), ('flags', ctypes.c_void_p)]
+
+
+class GroupedKernel:
+  def __init__(self, generators, threads=256, name=None):
+    if not generators:
+      raise GenerationError('a grouped launch needs at least one chain')
+    self.gens = generators
+    self.threads = threads
+    fp = {g.get_context().fp_type for g in generators}
+    if len(fp) != 1:
+      raise GenerationError('all groups of a grouped launch must use the same precision')
+    self.T = generators[0].get_context().fp_as_str()
+    self.fs = 8 if self.T == 'double' else 4
+    for g in generators:
+      if g.get_chain() is None:
+        g.generate()
+      if match_left_chain(g.get_chain()) is None:
+        raise GenerationError(f'{g.get_base_name()} is not a shared-left chain')
+      for t, stype in g.abi_symbols():
+        if t.addressing == Addressing.SCALAR:
+          raise GenerationError('scalar operands are not supported in grouped launches')
+      if len(g.abi_symbols()) > MAX_SYMBOLS:
+        raise GenerationError(f'at most {MAX_SYMBOLS} operands per group')
+    key = ','.join(g.get_base_name() for g in generators) + f'|{threads}'
+    self.name = name or 'grouped_' + hashlib.md5(key.encode()).hexdigest()[:10]
+    self._emit()
+    self._lib = None
+
+  def _emit(self):
+    parts, work_vals, a_vals, self.tiles_per = [], 0, 0, []
+    self.te = []
+    for gid, g in enumerate(self.gens):
+      shape = match_left_chain(g.get_chain())
+      plan = Plan('colprog', {'threads': self.threads, 'chunk': 16, 'a_source': 'smem', 'prefetch': 0})
+      em = _ColProg(g.get_chain(), shape, plan, g.get_context(), f'{self.name}_g{gid}')
+      parts.append(em.emit_group_functions(g.abi_symbols(), gid))
+      work_vals = max(work_vals, em.work_vals)
+      a_vals = max(a_vals, _pad(em.a_total, 4))
+      self.te.append(em.TE)
+    self.smem = (work_vals + a_vals) * self.fs
+    if self.smem > 227 * 1024:
+      raise GenerationError(f'grouped launch needs {self.smem} bytes of shared memory')
+    T, BT = self.T, self.threads
+    k = []
+    k.append(f'__global__ void __launch_bounds__({BT}) kernel_{self.name}(const tfb_group_args* __restrict__ args, '
+             'const uint2* __restrict__ items, unsigned num_items, unsigned* __restrict__ counter) {')
+    k.append('  extern __shared__ __align__(16) unsigned char tfb_smem_raw[];')
+    k.append(f'  {T}* const ubuf = reinterpret_cast<{T}*>(tfb_smem_raw);')
+    k.append(f'  {T}* const sA = ubuf + {work_vals};')
+    k.append('  __shared__ unsigned s_item;')
+    k.append('  int cur = -1;')
+    k.append('  for (;;) {')
+    k.append('    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1u);')
+    k.append('    __syncthreads();')
+    k.append('    const unsigned item = s_item;')
+    k.append('    __syncthreads();')
+    k.append('    if (item >= num_items) break;')
+    k.append('    const uint2 wi = items[item];')
+    k.append('    if ((int)wi.x != cur) {')
+    k.append('      switch (wi.x) {')
+    for gid in range(len(self.gens)):
+      k.append(f'        case {gid}u: group{gid}_stage_a(args[{gid}], sA); break;')
+    k.append('        default: break;')
+    k.append('      }')
+    k.append('      __syncthreads();')
+    k.append('      cur = (int)wi.x;')
+    k.append('    }')
+    k.append('    switch (wi.x) {')
+    for gid in range(len(self.gens)):
+      k.append(f'      case {gid}u: group{gid}_tile(args[{gid}], (size_t)wi.y, ubuf, sA); break;')
+    k.append('      default: break;')
+    k.append('    }')
+    k.append('    __syncthreads();')
+    k.append('  }')
+    k.append('}')
+    k.append('')
+    k.append(f'extern "C" int tfb_grouped_launch_{self.name}(const void* args, const void* items, unsigned num_items, '
+             'unsigned* counter, void* streamPtr) {')
+    k.append('  cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);')
+    k.append('  if (num_items == 0) return 0;')
+    k.append('  int device = 0, sms = 0, per = 0;')
+    k.append('  cudaGetDevice(&device);')
+    k.append('  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);')
+    k.append(f'  cudaFuncSetAttribute(kernel_{self.name}, cudaFuncAttributeMaxDynamicSharedMemorySize, {self.smem});')
+    k.append(f'  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel_{self.name}, {BT}, {self.smem});')
+    k.append('  unsigned grid = (unsigned)((per > 0 ? per : 1) * (sms > 0 ? sms : 1));')
+    k.append('  if (grid > num_items) grid = num_items;')
+    k.append('  cudaMemsetAsync(counter, 0, sizeof(unsigned), stream);')
+    k.append(f'  kernel_{self.name}<<<grid, {BT}, {self.smem}, stream>>>(static_cast<const tfb_group_args*>(args), '
+             'static_cast<const uint2*>(items), num_items, counter);')
+    k.append('  return (int)cudaGetLastError();')
+    k.append('}')
+    from .codegen import PRELUDE
+    self.source_text = PRELUDE + ARGS_STRUCT + '\n\n'.join(parts) + '\n\n' + '\n'.join(k) + '\n'
+
+  def source(self):
+    return self.source_text
+
+  def build(self):
+    self.so_path = build_library(self.source_text)
+    return self.so_path
+
+  def _load(self):
+    if self._lib is None:
+      self.build()
+      self._lib = ctypes.CDLL(self.so_path, mode=ctypes.RTLD_LOCAL)
+      self._fn = getattr(self._lib, f'tfb_grouped_launch_{self.name}')
+      self._fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint, ctypes.c_void_p, ctypes.c_void_p]
+      self._fn.restype = ctypes.c_int
+    return self._fn
+
+  def work_items(self, counts):
+    """(group, tile) pairs for element counts per group, ordered by group."""
+    items = []
+    for gid, n in enumerate(counts):
+      tiles = (int(n) + self.te[gid] - 1) // self.te[gid]
+      items.extend((gid, t) for t in range(tiles))
+    return items
+
+  def prepare(self, group_kwargs):
+    """Device argument records, work table and counter for one set of group buffers.
+
+    group_kwargs[g] maps group g's ABI names (as for CompiledKernel calls) to tensors /
+    addresses, plus numElements and optional flags. Returns a `GroupedLaunch`.
+    """
+    import torch
+    if len(group_kwargs) != len(self.gens):
+      raise ValueError('one argument set per group is required')
+    recs = (_GroupArgs * len(self.gens))()
+    keep = []
+    counts = []
+    for gid, (g, kw) in enumerate(zip(self.gens, group_kwargs)):
+      rec = recs[gid]
+      for i, (t, _) in enumerate(g.abi_symbols()):
+        v = kw[t.name]
+        rec.ptr[i] = v if isinstance(v, int) else int(v.data_ptr())
+        rec.off[i] = int(kw.get(f'{t.name}_extraOffset', 0))
+        keep.append(v)
+      rec.num_elements = int(kw['numElements'])
+      fl = kw.get('flags')
+      rec.flags = None if fl is None else int(fl.data_ptr())
+      if fl is not None:
+        keep.append(fl)
+      counts.append(int(kw['numElements']))
+    raw = bytes(recs)
+    dev_args = torch.frombuffer(bytearray(raw), dtype=torch.uint8).to('cuda')
+    items = self.work_items(counts)
+    dev_items = torch.tensor(items if items else [(0, 0)], dtype=torch.int32, device='cuda').contiguous()
+    counter = torch.zeros(1, dtype=torch.int32, device='cuda')
+    return GroupedLaunch(self, dev_args, dev_items, len(items), counter, keep)
+
+
+class GroupedLaunch:
+  """A prepared grouped launch; `launch()` runs it, `capture()` records it in a CUDA graph."""
+
+  def __init__(self, kernel, dev_args, dev_items, num_items, counter, keep):
+    self.kernel = kernel
+    self.dev_args = dev_args
+    self.dev_items = dev_items
+    self.num_items = num_items
+    self.counter = counter
+    self._keep = keep
+    self.graph = None
+
+  def launch(self, stream=None):
+    import torch
+    fn = self.kernel._load()
+    st = stream if stream is not None else torch.cuda.current_stream()
+    rc = fn(self.dev_args.data_ptr(), self.dev_items.data_ptr(), self.num_items, self.counter.data_ptr(),
+            st.cuda_stream)
+    if rc != 0:
+      raise RuntimeError(f'grouped launch failed with CUDA error {rc}')
+
+  def capture(self):
+    """Record launch (counter reset + persistent kernel) in a CUDA graph; returns the graph."""
+    import torch
+    self.kernel._load()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+      self.launch(s)            # warm-up outside capture (first-call attributes)
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+      self.launch(torch.cuda.current_stream())
+    self.graph = g
+    return g
+
+  def replay(self):
+    if self.graph is None:
+      self.capture()
+    self.graph.replay()

@@ -57,3 +57,23 @@ def catalogue():
   for case, fp, opts in EXTRA:
     add(case, fp, opts)
   return out
+
+
+def grouped_catalogue():
+  """Grouped (mixed-shape) kernels used by the tests and the benchmark."""
+  from oracle import cases
+  from .grouped import GroupedKernel
+  ns = cases.ns_from_module('tensorforge_b200')
+  out = []
+  sets = {
+    'test': [(10, 9), (20, 27), (35, 9), (56, 9), (84, 27)],
+    'bench_c3': [(b, q) for b, q, _ in cases.mixed_shape_groups()],
+  }
+  for tag, shapes in sets.items():
+    gens = []
+    for b, q in shapes:
+      g = Generator(cases.mixed_chain(ns, b, q), Context('sm_100a', 'cuda', FP['float']))
+      g.generate()
+      gens.append(g)
+    out.append((tag, GroupedKernel(gens)))
+  return out

@@ -147,7 +147,7 @@ def r_slots(term):
 
 def colprog_plan(chain, shape: LeftChain, fp_size, variant):
   from ..codegen.colprog import tile_elements
-  threads = variant.get('threads', 256)
+  threads = variant.get('threads', 128)
   chunk = variant.get('chunk', 16)
   a_source = variant.get('a_source', 'const')
   vec = 4 if fp_size == 4 else 2
@@ -167,8 +167,15 @@ def colprog_plan(chain, shape: LeftChain, fp_size, variant):
     smem += (a_vals + vec) * fp_size
   if smem > SMEM_LIMIT:
     return None
+  prefetch = int(variant.get('prefetch', 1))
+  if prefetch:
+    smem += sum(te * ((op.storage_size() if op.sparse else op.element_volume()) + vec - 1) // vec * vec
+                for op in {id(o): o for t in shape.terms for o in (t.B, t.R)
+                           if o is not None and o.kind == 'batched'}.values()) * fp_size
+    if smem > SMEM_LIMIT:
+      prefetch = 0
   return Plan('colprog', {'threads': threads, 'chunk': chunk, 'min_blocks': variant.get('min_blocks', 0),
-                          'a_source': a_source},
+                          'a_source': a_source, 'prefetch': prefetch},
               smem, threads, note=f'M={shape.M} N={shape.N} terms={len(shape.terms)} tile={te}')
 
 
