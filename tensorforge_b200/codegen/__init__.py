@@ -19,6 +19,7 @@ PRELUDE = '''#include <cuda_runtime.h>
 #include <cstddef>
 #include <atomic>
 #include <mutex>
+#include <cstdio>
 #include "tensorforge_aux.h"
 '''
 

@@ -33,16 +33,8 @@ from .runtime.build import build_library
 
 MAX_SYMBOLS = 16
 
-ARGS_STRUCT = f'''
-#ifndef TFB_GROUP_ARGS
-#define TFB_GROUP_ARGS
-struct tfb_group_args {{
-  const void* ptr[{MAX_SYMBOLS}];
-  unsigned off[{MAX_SYMBOLS}];
-  unsigned long long num_elements;
-  const unsigned* flags;
-}};
-#endif
+ARGS_STRUCT = '''
+#include "tensorforge_b200_grouped.h"
 '''
 
 
@@ -141,8 +133,128 @@ class GroupedKernel:
              'static_cast<const uint2*>(items), num_items, counter);')
     k.append('  return (int)cudaGetLastError();')
     k.append('}')
+    k += self._noalloc_variant(work_vals)
     from .codegen import PRELUDE
     self.source_text = PRELUDE + ARGS_STRUCT + '\n\n'.join(parts) + '\n\n' + '\n'.join(k) + '\n'
+
+  def _noalloc_variant(self, work_vals):
+    """An entry point for callers that cannot allocate device memory.
+
+    Some callers cannot call cudaMalloc: code running where the device allocator is off
+    limits (inside a host callback, under an external memory manager that owns every
+    allocation, or in a tight real-time loop where an allocation could block). For them
+    this variant keeps its scratch - the work counter, the per-group tile offsets and the
+    group argument records - in a file-scope device array of fixed size instead of
+    caller-provided buffers; the caller still passes every input and output.
+    """
+    T, BT, G = self.T, self.threads, len(self.gens)
+    te = ', '.join(str(t) for t in self.te)
+    k = ['',
+         '// Scratch of the allocation-free entry point: every GPU that loads this library keeps',
+         '// one copy until the process exits. All calls share it and it keeps the last call\'s',
+         '// contents, so calls that overlap on the GPU (different streams, no ordering) race.',
+         'struct tfb_noalloc_scratch {',
+         '  unsigned counter;',
+         '  unsigned num_groups;',
+         '  unsigned tile_prefix[TFB_NOALLOC_MAX_GROUPS + 1];',
+         '  tfb_group_args args[TFB_NOALLOC_MAX_GROUPS];',
+         '};',
+         'static __device__ __align__(256) unsigned char tfb_noalloc_scratch_storage[sizeof(tfb_noalloc_scratch)];',
+         '',
+         f'__global__ void __launch_bounds__({BT}) kernel_{self.name}_noalloc(const tfb_noalloc_scratch* __restrict__ scr, '
+         'unsigned* __restrict__ counter) {',
+         '  extern __shared__ __align__(16) unsigned char tfb_smem_raw[];',
+         f'  {T}* const ubuf = reinterpret_cast<{T}*>(tfb_smem_raw);',
+         f'  {T}* const sA = ubuf + {work_vals};',
+         '  __shared__ unsigned s_item, s_group, s_tile;',
+         '  const unsigned ngroups = scr->num_groups;',
+         '  const unsigned total = scr->tile_prefix[ngroups];',
+         '  int cur = -1;',
+         '  for (;;) {',
+         '    if (threadIdx.x == 0) {',
+         '      const unsigned item = atomicAdd(counter, 1u);',
+         '      unsigned g = 0;',
+         '      while (g + 1u < ngroups && scr->tile_prefix[g + 1u] <= item) ++g;',
+         '      s_item = item; s_group = g; s_tile = item - scr->tile_prefix[g];',
+         '    }',
+         '    __syncthreads();',
+         '    const unsigned item = s_item, grp = s_group, tile = s_tile;',
+         '    __syncthreads();',
+         '    if (item >= total) break;',
+         '    if ((int)grp != cur) {',
+         '      switch (grp) {']
+    for gid in range(G):
+      k.append(f'        case {gid}u: group{gid}_stage_a(scr->args[{gid}], sA); break;')
+    k += ['        default: break;',
+          '      }',
+          '      __syncthreads();',
+          '      cur = (int)grp;',
+          '    }',
+          '    switch (grp) {']
+    for gid in range(G):
+      k.append(f'      case {gid}u: group{gid}_tile(scr->args[{gid}], (size_t)tile, ubuf, sA); break;')
+    k += ['      default: break;',
+          '    }',
+          '    __syncthreads();',
+          '  }',
+          '}',
+          '',
+          '// Allocation-free form of tfb_grouped_launch_<set>: the group records are read from host',
+          '// memory (`host_args`, num_groups of them, in group order) and copied into the static',
+          '// scratch on `stream`; the work counter there is cleared by the same copy. Allocates',
+          '// nothing. The first call on a device looks up the scratch address for that device',
+          '// (do it before any stream capture). Returns a cudaError_t value;',
+          '// cudaErrorInvalidValue when num_groups exceeds the fused set or TFB_NOALLOC_MAX_GROUPS.',
+          f'extern "C" int tfb_grouped_launch_noalloc_{self.name}(const void* host_args, unsigned num_groups, void* streamPtr) {{',
+          f'  static const unsigned tiles_per_group[{G}] = {{{te}}};',
+          '  static void* scratch_ptr[64];',
+          '  static std::mutex setup_mu;',
+          '  cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);',
+          f'  if (num_groups > {G}u || num_groups > TFB_NOALLOC_MAX_GROUPS || host_args == nullptr) {{',
+          f'    std::fprintf(stderr, "tfb_grouped_launch_noalloc_{self.name}: %u groups requested, at most {min(G, 64)} supported\\n", num_groups);',
+          '    return (int)cudaErrorInvalidValue;',
+          '  }',
+          '  if (num_groups == 0) return 0;',
+          '  int device = 0;',
+          '  cudaError_t err = cudaGetDevice(&device);',
+          '  if (err != cudaSuccess) return (int)err;',
+          '  if (device < 0 || device >= 64) return (int)cudaErrorInvalidDevice;',
+          '  {',
+          '    std::lock_guard<std::mutex> guard(setup_mu);',
+          '    if (scratch_ptr[device] == nullptr) {',
+          '      void* p = nullptr;',
+          '      err = cudaGetSymbolAddress(&p, tfb_noalloc_scratch_storage);',
+          '      if (err != cudaSuccess) return (int)err;',
+          '      scratch_ptr[device] = p;',
+          '    }',
+          '  }',
+          '  tfb_noalloc_scratch host{};',
+          '  host.counter = 0u;',
+          '  host.num_groups = num_groups;',
+          '  const tfb_group_args* ga = static_cast<const tfb_group_args*>(host_args);',
+          '  unsigned long long total = 0;',
+          '  for (unsigned g = 0; g < num_groups; ++g) {',
+          '    host.args[g] = ga[g];',
+          '    host.tile_prefix[g] = (unsigned)total;',
+          '    total += (ga[g].num_elements + tiles_per_group[g] - 1) / tiles_per_group[g];',
+          '  }',
+          '  if (total > 0xFFFFFFF0ull) return (int)cudaErrorInvalidValue;',
+          '  host.tile_prefix[num_groups] = (unsigned)total;',
+          '  if (total == 0) return 0;',
+          '  // pageable source: the copy is staged before this call returns, so `host` may go',
+          '  err = cudaMemcpyAsync(scratch_ptr[device], &host, sizeof(host), cudaMemcpyHostToDevice, stream);',
+          '  if (err != cudaSuccess) return (int)err;',
+          '  int sms = 0, per = 0;',
+          '  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);',
+          f'  cudaFuncSetAttribute(kernel_{self.name}_noalloc, cudaFuncAttributeMaxDynamicSharedMemorySize, {self.smem});',
+          f'  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel_{self.name}_noalloc, {BT}, {self.smem});',
+          '  unsigned grid = (unsigned)((per > 0 ? per : 1) * (sms > 0 ? sms : 1));',
+          '  if (grid > total) grid = (unsigned)total;',
+          '  tfb_noalloc_scratch* scr = static_cast<tfb_noalloc_scratch*>(scratch_ptr[device]);',
+          f'  kernel_{self.name}_noalloc<<<grid, {BT}, {self.smem}, stream>>>(scr, &scr->counter);',
+          '  return (int)cudaGetLastError();',
+          '}']
+    return k
 
   def source(self):
     return self.source_text
@@ -199,6 +311,35 @@ class GroupedKernel:
     dev_items = torch.tensor(items if items else [(0, 0)], dtype=torch.int32, device='cuda').contiguous()
     counter = torch.zeros(1, dtype=torch.int32, device='cuda')
     return GroupedLaunch(self, dev_args, dev_items, len(items), counter, keep)
+
+
+def host_records(kernel, group_kwargs):
+  """tfb_group_args records in host memory (for the allocation-free entry point)."""
+  recs = (_GroupArgs * len(group_kwargs))()
+  for gid, (g, kw) in enumerate(zip(kernel.gens, group_kwargs)):
+    rec = recs[gid]
+    for i, (t, _) in enumerate(g.abi_symbols()):
+      v = kw[t.name]
+      rec.ptr[i] = v if isinstance(v, int) else int(v.data_ptr())
+      rec.off[i] = int(kw.get(f'{t.name}_extraOffset', 0))
+    rec.num_elements = int(kw['numElements'])
+    fl = kw.get('flags')
+    rec.flags = None if fl is None else int(fl.data_ptr())
+  return recs
+
+
+def launch_noalloc(kernel, group_kwargs, stream=None):
+  """Call tfb_grouped_launch_noalloc_<set>: no device allocation by this call or the library."""
+  import torch
+  kernel._load()
+  fn = getattr(kernel._lib, f'tfb_grouped_launch_noalloc_{kernel.name}')
+  fn.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_void_p]
+  fn.restype = ctypes.c_int
+  recs = host_records(kernel, group_kwargs)
+  st = stream if stream is not None else torch.cuda.current_stream()
+  rc = fn(ctypes.addressof(recs), len(group_kwargs), st.cuda_stream)
+  if rc != 0:
+    raise RuntimeError(f'allocation-free grouped launch failed with CUDA error {rc}')
 
 
 class GroupedLaunch:
