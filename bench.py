@@ -227,7 +227,7 @@ def impl_reference(args, rank, world):
 def extra_workloads(stream, short=False):
   """Secondary BASELINE configs measured next to the headline (device-resident inputs)."""
   import torch
-  from oracle import cases
+  from tensorforge_b200 import workloads as cases
   from tensorforge_b200.kernels import make
   from tensorforge_b200.runtime import compile_generator
   out = {}
@@ -297,7 +297,7 @@ def extra_workloads(stream, short=False):
 
 def impl_ours(args, rank, world, dist):
   import torch
-  from oracle import cases
+  from tensorforge_b200 import workloads as cases
   from tensorforge_b200.kernels import make
   from tensorforge_b200.runtime import compile_generator
   from tensorforge_b200.common.basic_types import DataFlowDirection

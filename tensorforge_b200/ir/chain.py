@@ -75,9 +75,9 @@ class Operand:
     Entries outside the pattern's index mask are absent (value 0), matching
     `ListSPP.linear_index` returning None (spp.py:102-107).
     """
-    out = {}
-    for idx, pos in self.nonzeros():
-      out[idx] = pos
+    out = self.__dict__.get('_lookup')
+    if out is None:  # built once: the pattern of an operand never changes after lowering
+      out = self.__dict__['_lookup'] = {idx: pos for idx, pos in self.nonzeros()}
     return out
 
 

@@ -24,7 +24,7 @@ EXTRA = [
 
 
 def make(case, fp='float', **opts):
-  from oracle import cases  # the case catalogue is shared with the tests
+  from . import workloads as cases
   ns = cases.ns_from_module('tensorforge_b200')
   g = Generator(cases.build(case, ns), Context('sm_100a', 'cuda', FP[fp], Options(**opts)))
   g.generate()
@@ -61,7 +61,7 @@ def catalogue():
 
 def grouped_catalogue():
   """Grouped (mixed-shape) kernels used by the tests and the benchmark."""
-  from oracle import cases
+  from . import workloads as cases
   from .grouped import GroupedKernel
   ns = cases.ns_from_module('tensorforge_b200')
   out = []

@@ -145,6 +145,12 @@ def r_slots(term):
   return [[(m, j * P + m) for m in range(P)] for j in range(N)]
 
 
+# Column programs unroll one FMA per nonzero of every A_t into straight-line code. Above
+# this many the instruction stream outgrows the SM's instruction caches and ptxas time grows
+# to minutes per kernel, so such chains go to the generic generator.
+COLPROG_MAX_FMAS = 6144
+
+
 def colprog_plan(chain, shape: LeftChain, fp_size, variant):
   from ..codegen.colprog import tile_elements
   threads = variant.get('threads', 128)
@@ -153,6 +159,8 @@ def colprog_plan(chain, shape: LeftChain, fp_size, variant):
   vec = 4 if fp_size == 4 else 2
   chunk = max(vec, (chunk + vec - 1) // vec * vec)
   if shape.M > 128 or shape.N > threads:
+    return None
+  if sum(t.A.storage_size() for t in shape.terms) > COLPROG_MAX_FMAS:
     return None
   te = tile_elements(shape, threads)
   kmax = max(t.K for t in shape.terms)

@@ -71,19 +71,26 @@ def build_library(source, extra_flags=(), verbose_ptxas=False):
   so = library_path(source, extra_flags)
   if os.path.exists(so):
     return so
-  with _lock:
-    if os.path.exists(so):
-      return so
+  with _lock:  # the shared helper object is built once; libraries build concurrently
     os.makedirs(CACHE, exist_ok=True)
-    cu = so[:-3] + '.cu'
-    with open(cu, 'w') as f:
-      f.write(source)
     aux = aux_object()
-    flags = list(extra_flags) + (['-Xptxas', '-v'] if verbose_ptxas else [])
-    tmp = so + f'.{os.getpid()}.tmp.so'
+  # per-process, per-thread temporaries + atomic rename: concurrent builders of the same
+  # source (threads or processes) each produce a complete file and the last rename wins
+  tag = f'{os.getpid()}.{threading.get_ident()}'
+  cu = so[:-3] + f'.{tag}.cu'
+  with open(cu, 'w') as f:
+    f.write(source)
+  flags = list(extra_flags) + (['-Xptxas', '-v'] if verbose_ptxas else [])
+  tmp = so + f'.{tag}.tmp.so'
+  try:
     _run([nvcc()] + ARCH_FLAGS + BASE_FLAGS + flags + [f'-I{INCLUDE}', '-shared', cu, aux, '-o', tmp, '-lcuda'],
          so[:-3] + '.log')
     os.replace(tmp, so)
+    os.replace(cu, so[:-3] + '.cu')
+  finally:
+    for path in (cu, tmp):
+      if os.path.exists(path):
+        os.remove(path)
   return so
 
 

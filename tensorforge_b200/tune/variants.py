@@ -1,0 +1,88 @@
+"""Tunable variants of a chain and the cost model's 32-dim feature vectors."""
+import math
+
+from ..plan import SMEM_LIMIT
+from ..plan.chains import match_left_chain
+
+GENERIC_G = (4, 8, 16, 32, 64)
+GENERIC_E = (1, 2, 4, 8, 16)
+COLPROG = [dict(threads=t, a_source=a) for t in (128, 256) for a in ("const", "smem")]
+NFEAT = 32
+TUNE_COLPROG_MAX_FMAS = 2048
+
+
+def variant_space(chain, fp_size=4):
+  """Variant dicts (Options.variant) that apply to `chain`."""
+  from ..codegen.generic import smem_layout
+  out = []
+  shared, per_elem = smem_layout(chain)
+  for g in GENERIC_G:
+    for e in GENERIC_E:
+      if g * e > 1024 or g * e < 32:
+        continue
+      if (shared + per_elem * e) * fp_size > SMEM_LIMIT:
+        continue
+      out.append({'strategy': 'generic', 'threads_per_element': g, 'elements_per_block': e})
+  shape = match_left_chain(chain)
+  if shape is not None and shape.M <= 128 and shape.N <= 128:
+    # tuning builds every variant; column programs with large A cost ptxas close to a
+    # minute each, so only the planner's own column program is measured for those
+    if sum(t.A.storage_size() for t in shape.terms) <= TUNE_COLPROG_MAX_FMAS:
+      for v in COLPROG:
+        if shape.N <= v['threads']:
+          out.append(dict(strategy='colprog', **v))
+  return out
+
+
+def _l2(x):
+  return math.log2(max(1.0, float(x)))
+
+
+def chain_features(spec, chain):
+  """20 features of the chain itself."""
+  f = [len(spec.stages) / 4.0]
+  for i in range(4):
+    if i < len(spec.stages):
+      s = spec.stages[i]
+      f += [_l2(s.rows) / 7.0, _l2(s.cols) / 7.0, _l2(s.k) / 7.0, s.density]
+    else:
+      f += [0.0, 0.0, 0.0, 0.0]
+  f.append(math.log10(spec.batch) / 6.0)
+  f.append(math.log10(max(1.0, chain.nz_flops_per_element())) / 7.0)
+  f.append(math.log10(max(1.0, chain.bytes_per_element())) / 6.0)
+  return f
+
+
+def variant_features(chain, variant, fp_size=4):
+  """12 features of the variant (strategy, launch shape, shared memory).
+
+  `variant` holds the parameters the planner actually applied (the plan's params plus
+  'strategy'), not the requested ones: a requested constant-memory A that does not fit
+  falls back to shared memory, for example.
+  """
+  from ..codegen.generic import smem_layout
+  shared, per_elem = smem_layout(chain)
+  if variant['strategy'] == 'generic':
+    g, e = variant['threads_per_element'], variant['elements_per_block']
+    smem = (shared + per_elem * e) * fp_size
+    return [1.0, 0.0, _l2(g) / 6.0, _l2(e) / 4.0, g * e / 1024.0, 0.0, 0.0, smem / SMEM_LIMIT,
+            math.log10(max(1, per_elem * fp_size)) / 5.0, 0.0, 0.0, 0.0]
+  t = variant['threads']
+  shape = match_left_chain(chain)
+  te = max(1, t // shape.N)
+  return [0.0, 1.0, 0.0, _l2(te) / 6.0, t / 1024.0, 1.0 if variant['a_source'] == 'const' else 0.0,
+          te * shape.N / t, 0.0, 0.0, shape.M / 128.0, len(shape.terms) / 4.0, 0.0]
+
+
+def features(spec, chain, variant):
+  cf = getattr(chain, '_tune_features', None)
+  if cf is None:  # the chain part is shared by all variants (and costs a nonzero count)
+    cf = chain._tune_features = chain_features(spec, chain)
+  f = cf + variant_features(chain, variant)
+  assert len(f) == NFEAT, len(f)
+  return f
+
+
+def effective_variant(plan):
+  """The variant dict a plan realises (its strategy and applied parameters)."""
+  return dict(strategy=plan.strategy, **plan.params)

@@ -1,0 +1,218 @@
+"""Named descriptor chains: the benchmark workloads and the parity cases.
+
+Every builder takes a namespace `ns` exposing the TensorForge frontend names (`Tensor`,
+`SubTensor`, `BoundingBox`, `ListSPP`, `Addressing`, `MultilinearDescr`, `GemmDescr`,
+`generate_tmp_tensor`), so the same chain can be built with the reference package and
+with tensorforge_b200 and the two results compared on identical inputs. Builders only
+describe inputs; they compute nothing. Shapes follow the reference's own test suites and
+benchmark programs: tests/gemms/testsuites/*.yaml, benchmarks/fused/programs/s3time.cf,
+benchmarks/simple-gemm/params.yaml.
+"""
+import numpy as np
+
+
+def sparse_pattern(rows, cols, density, seed):
+  """Seeded Bernoulli pattern, entries listed in column-major order."""
+  rng = np.random.default_rng(seed)
+  mask = rng.random((rows, cols)) < density
+  return [(int(i), int(j)) for j in range(cols) for i in range(rows) if mask[i, j]]
+
+
+def fixed_nnz_pattern(rows, cols, nnz, seed):
+  """Seeded pattern with exactly `nnz` entries, column-major order."""
+  rng = np.random.default_rng(seed)
+  flat = np.sort(rng.choice(rows * cols, size=nnz, replace=False))
+  ij = [(int(f % rows), int(f // rows)) for f in flat]
+  return sorted(ij, key=lambda t: (t[1], t[0]))
+
+
+def ns_from_module(root):
+  """Namespace of frontend names from a package root ('tensorforge' or 'tensorforge_b200')."""
+  import importlib
+  tm = importlib.import_module(f'{root}.common.matrix.tensor')
+  bb = importlib.import_module(f'{root}.common.matrix.boundingbox')
+  sp = importlib.import_module(f'{root}.common.matrix.spp')
+  bt = importlib.import_module(f'{root}.common.basic_types')
+  de = importlib.import_module(f'{root}.generators.descriptions')
+  ax = importlib.import_module(f'{root}.common.aux')
+
+  class NS:
+    pass
+  ns = NS()
+  ns.Tensor, ns.SubTensor = tm.Tensor, tm.SubTensor
+  ns.BoundingBox = bb.BoundingBox
+  ns.ListSPP, ns.MaskSPP, ns.FullSPP = sp.ListSPP, sp.MaskSPP, sp.FullSPP
+  ns.Addressing = bt.Addressing
+  ns.FloatingPointType = bt.FloatingPointType
+  ns.MultilinearDescr, ns.GemmDescr = de.MultilinearDescr, de.GemmDescr
+  ns.generate_tmp_tensor = ax.generate_tmp_tensor
+  return ns
+
+
+# --------------------------------------------------------------------------- chains
+
+def plain_gemm(ns, m=56, k=56, n=9, addr_b='pointer_based', addr_c='pointer_based',
+               addr_a='none', add=False, alpha=1.0):
+  """C_e = A * B_e (BASELINE config 0 when m=k=56, n=9, B/C pointer arrays)."""
+  A = ns.Tensor([m, k], ns.Addressing.str2addr(addr_a))
+  B = ns.Tensor([k, n], ns.Addressing.str2addr(addr_b))
+  C = ns.Tensor([m, n], ns.Addressing.str2addr(addr_c))
+  if alpha != 1.0:
+    return [ns.GemmDescr(False, False, ns.SubTensor(A), ns.SubTensor(B), ns.SubTensor(C), alpha=alpha)]
+  return [ns.MultilinearDescr(ns.SubTensor(C), [ns.SubTensor(A), ns.SubTensor(B)],
+                              [[0, -1], [-1, 1]], [[0, 1], [0, 1]], add=add)]
+
+
+def volume_chain(ns, basis=56, quantities=9, terms=3, k_density=0.45, s_nnz=24, seed=0,
+                 k_addr='none', q_addr='strided', s_addr='strided', out_addr='strided'):
+  """out_e = sum_t K_t * Q_e * S_{e,t} (s3time.cf).
+
+  K_t: shared sparse basis x basis (ListSPP, seeded Bernoulli(k_density) pattern).
+  S_{e,t}: per-element sparse quantities x quantities with `s_nnz` seeded nonzeros,
+  strided with the full q*q slot per element, values stored compactly at its start.
+  """
+  Q = ns.Tensor([basis, quantities], ns.Addressing.str2addr(q_addr))
+  out = ns.Tensor([basis, quantities], ns.Addressing.str2addr(out_addr))
+  descrs = []
+  for t in range(terms):
+    kp = sparse_pattern(basis, basis, k_density, seed * 1000 + 11 + t)
+    sp = fixed_nnz_pattern(quantities, quantities, min(s_nnz, quantities * quantities), seed * 1000 + 101 + t)
+    K = ns.Tensor([basis, basis], ns.Addressing.str2addr(k_addr),
+                  spp=ns.ListSPP(kp, (basis, basis)) if k_density < 1.0 else None)
+    S = ns.Tensor([quantities, quantities], ns.Addressing.str2addr(s_addr),
+                  spp=ns.ListSPP(sp, (quantities, quantities)) if s_nnz < quantities * quantities else None)
+    T = ns.generate_tmp_tensor([ns.SubTensor(K), ns.SubTensor(Q)], [[0, -1], [-1, 1]])
+    descrs.append(ns.MultilinearDescr(ns.SubTensor(T), [ns.SubTensor(K), ns.SubTensor(Q)],
+                                      [[0, -1], [-1, 1]], [[0, 1], [0, 1]]))
+    descrs.append(ns.MultilinearDescr(ns.SubTensor(out), [ns.SubTensor(T), ns.SubTensor(S)],
+                                      [[0, -1], [-1, 1]], [[0, 1], [0, 1]], add=(t > 0)))
+  return descrs
+
+
+def subbox_gemm(ns, box_a, box_b, box_c, shape=56, addr='strided', trans_a=False, trans_b=False):
+  """Sub-bounding-box GEMMs from tests/gemms/testsuites/notrans-notrans-tests.yaml:1-35."""
+  BB = ns.BoundingBox
+  A = ns.Tensor([shape, shape], ns.Addressing.str2addr(addr), BB(box_a[:2], box_a[2:]))
+  B = ns.Tensor([shape, shape], ns.Addressing.str2addr(addr), BB(box_b[:2], box_b[2:]))
+  C = ns.Tensor([shape, shape], ns.Addressing.str2addr(addr), BB(box_c[:2], box_c[2:]))
+  return [ns.GemmDescr(trans_a, trans_b, ns.SubTensor(A), ns.SubTensor(B), ns.SubTensor(C))]
+
+
+def three_matrices(ns):
+  """D += A x (B x C) with a temporary (example/three_matrices.py:9-32)."""
+  BB = ns.BoundingBox
+  D = ns.Tensor([56, 9], ns.Addressing.STRIDED, BB([0, 0], [56, 9]))
+  A = ns.Tensor([56, 56], ns.Addressing.STRIDED, BB([0, 0], [56, 56]))
+  B = ns.Tensor([56, 9], ns.Addressing.STRIDED, BB([0, 0], [56, 9]))
+  C = ns.Tensor([9, 9], ns.Addressing.STRIDED, BB([0, 0], [9, 9]))
+  T = ns.generate_tmp_tensor([ns.SubTensor(B), ns.SubTensor(C)], [[0, -1], [-1, 1]])
+  return [ns.MultilinearDescr(ns.SubTensor(T), [ns.SubTensor(B), ns.SubTensor(C)], [[0, -1], [-1, 1]], [[0, 1], [0, 1]]),
+          ns.MultilinearDescr(ns.SubTensor(D), [ns.SubTensor(A), ns.SubTensor(T)], [[0, -1], [-1, 1]], [[0, 1], [0, 1]], add=True)]
+
+
+def sparse_dense(ns, m=20, k=20, n=9, density=0.3, seed=5, sparse_side='a', addr_sparse='none'):
+  """Sparse x dense and dense x sparse GEMMs (tests/{sparse_dense,dense_sparse}_gemms)."""
+  if sparse_side == 'a':
+    pat = sparse_pattern(m, k, density, seed)
+    A = ns.Tensor([m, k], ns.Addressing.str2addr(addr_sparse), spp=ns.ListSPP(pat, (m, k)))
+    B = ns.Tensor([k, n], ns.Addressing.STRIDED)
+  else:
+    pat = sparse_pattern(k, n, density, seed)
+    A = ns.Tensor([m, k], ns.Addressing.NONE)
+    B = ns.Tensor([k, n], ns.Addressing.str2addr(addr_sparse), spp=ns.ListSPP(pat, (k, n)))
+  C = ns.Tensor([m, n], ns.Addressing.STRIDED)
+  return [ns.MultilinearDescr(ns.SubTensor(C), [ns.SubTensor(A), ns.SubTensor(B)], [[0, -1], [-1, 1]], [[0, 1], [0, 1]])]
+
+
+def rank3(ns):
+  """dest[i,j,l] = sum_k A[i,k] * B[k,j,l] (a general multilinear product)."""
+  A = ns.Tensor([10, 6], ns.Addressing.NONE)
+  B = ns.Tensor([6, 5, 4], ns.Addressing.STRIDED)
+  D = ns.Tensor([10, 5, 4], ns.Addressing.STRIDED)
+  return [ns.MultilinearDescr(ns.SubTensor(D), [ns.SubTensor(A), ns.SubTensor(B)],
+                              [[0, -1], [-1, 1, 2]], [[0, 1], [0, 1, 2]])]
+
+
+def two_contractions(ns):
+  """dest[i,j] = sum_{k,l} A[i,k,l] * B[k,l,j] (two contracted indices)."""
+  A = ns.Tensor([8, 4, 3], ns.Addressing.NONE)
+  B = ns.Tensor([4, 3, 7], ns.Addressing.PTR_BASED)
+  D = ns.Tensor([8, 7], ns.Addressing.PTR_BASED)
+  return [ns.MultilinearDescr(ns.SubTensor(D), [ns.SubTensor(A), ns.SubTensor(B)],
+                              [[0, -1, -2], [-1, -2, 1]], [[0, 1, 2], [0, 1, 2]])]
+
+
+def scalar_scaled(ns):
+  """dest[i,j] = A[i,k] * B[k,j] * s with a SCALAR operand passed by value."""
+  A = ns.Tensor([16, 12], ns.Addressing.NONE)
+  B = ns.Tensor([12, 5], ns.Addressing.STRIDED)
+  S = ns.Tensor([], ns.Addressing.SCALAR)
+  D = ns.Tensor([16, 5], ns.Addressing.STRIDED)
+  return [ns.MultilinearDescr(ns.SubTensor(D), [ns.SubTensor(A), ns.SubTensor(B), ns.SubTensor(S)],
+                              [[0, -1], [-1, 1], []], [[0, 1], [0, 1], []])]
+
+
+def outer_product(ns):
+  """dest[i,j] = a[i] * b[j] (no contraction)."""
+  a = ns.Tensor([13], ns.Addressing.STRIDED)
+  b = ns.Tensor([7], ns.Addressing.NONE)
+  D = ns.Tensor([13, 7], ns.Addressing.STRIDED)
+  return [ns.MultilinearDescr(ns.SubTensor(D), [ns.SubTensor(a), ns.SubTensor(b)], [[0], [1]], [[0], [0]])]
+
+
+CASES = {
+  # name: (builder, kwargs, num_elements)
+  'c0_gemm_ptr': (plain_gemm, {}, 24),
+  'c0_gemm_strided': (plain_gemm, {'addr_b': 'strided', 'addr_c': 'strided'}, 16),
+  'gemm_add': (plain_gemm, {'m': 24, 'k': 17, 'n': 5, 'addr_b': 'strided', 'addr_c': 'strided', 'add': True}, 16),
+  'gemm_alpha': (plain_gemm, {'m': 12, 'k': 8, 'n': 4, 'addr_b': 'strided', 'addr_c': 'strided', 'alpha': 1.5}, 8),
+  'gemm_batched_a': (plain_gemm, {'m': 33, 'k': 9, 'n': 11, 'addr_a': 'strided', 'addr_b': 'strided', 'addr_c': 'strided'}, 16),
+  'chain_o6': (volume_chain, {}, 16),
+  'chain_o4_q27': (volume_chain, {'basis': 20, 'quantities': 27, 's_nnz': 72, 'seed': 3}, 16),
+  'chain_o3_dense': (volume_chain, {'basis': 10, 'quantities': 9, 'k_density': 1.0, 's_nnz': 81, 'seed': 1, 'terms': 2}, 16),
+  'subbox_0': (subbox_gemm, {'box_a': [0, 0, 33, 9], 'box_b': [0, 0, 9, 11], 'box_c': [0, 0, 33, 11]}, 3),
+  'subbox_1': (subbox_gemm, {'box_a': [22, 46, 55, 55], 'box_b': [46, 44, 55, 55], 'box_c': [0, 44, 33, 55]}, 3),
+  'subbox_2': (subbox_gemm, {'box_a': [11, 23, 44, 32], 'box_b': [23, 22, 32, 33], 'box_c': [11, 22, 44, 33]}, 3),
+  'trans_a': (subbox_gemm, {'box_a': [0, 0, 20, 20], 'box_b': [0, 0, 20, 7], 'box_c': [0, 0, 20, 7], 'shape': 20, 'trans_a': True}, 8),
+  'three_matrices': (three_matrices, {}, 5),
+  'sparse_a_shared': (sparse_dense, {'sparse_side': 'a'}, 16),
+  'sparse_a_batched': (sparse_dense, {'sparse_side': 'a', 'addr_sparse': 'strided'}, 16),
+  'sparse_b_batched': (sparse_dense, {'sparse_side': 'b', 'addr_sparse': 'strided'}, 16),
+  'rank3': (rank3, {}, 8),
+  'two_contractions': (two_contractions, {}, 8),
+  'scalar_scaled': (scalar_scaled, {}, 8),
+  'outer_product': (outer_product, {}, 8),
+}
+
+
+def build(name, ns):
+  fn, kwargs, _ = CASES[name]
+  return fn(ns, **kwargs)
+
+
+def num_elements(name):
+  return CASES[name][2]
+
+
+MIXED_BASES = (10, 20, 35, 56, 84)
+MIXED_QUANTITIES = (9, 27)
+
+
+def mixed_shape_groups(total=1_500_000, seed=0, lo=1_000, hi=200_000):
+  """basis sizes {10,20,35,56,84} x quantity counts {9,27}.
+
+  Returns [(basis, quantities, element count)], counts drawn log-uniform over lo..hi from
+  `seed`, rescaled to sum to ~`total`, each rounded to a multiple of 8.
+  """
+  rng = np.random.default_rng(seed)
+  shapes = [(b, q) for b in MIXED_BASES for q in MIXED_QUANTITIES]
+  raw = np.exp(rng.uniform(np.log(lo), np.log(hi), len(shapes)))
+  raw = raw * (total / raw.sum())
+  counts = [max(8, int(round(c / 8)) * 8) for c in raw]
+  return [(b, q, c) for (b, q), c in zip(shapes, counts)]
+
+
+def mixed_chain(ns, basis, quantities, seed=0):
+  """The order-`basis` volume chain with patterns seeded per shape (S density ~30%)."""
+  nnz = max(1, int(round(0.3 * quantities * quantities)))
+  return volume_chain(ns, basis=basis, quantities=quantities, s_nnz=nnz, seed=seed * 100 + basis * 7 + quantities)
