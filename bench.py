@@ -281,7 +281,7 @@ def extra_workloads(stream, short=False):
                             'separate_launches_ms': ms2, 'separate_elements_per_s': total_el / (ms2 / 1e3)}
   # FP64 order-6 chain
   n = 100000 if short else 500000
-  for label, opts in (('fp64_plain', {}),):
+  for label, opts in (('fp64_plain', {}), ('fp64_dmma', {'precision': 'dmma'})):
     g = make(CASE, 'double', **opts)
     k = compile_generator(g)
     kw = {'numElements': n}
@@ -291,7 +291,8 @@ def extra_workloads(stream, short=False):
     total, per = time_launches(lambda: k(**kw), stream, 5, 2)
     ms = sum(per) / len(per)
     out[f'chain_o6_{label}'] = {'elements_per_s': n / (ms / 1e3), 'plan': g.get_plan().key(), 'elements': n,
-                                'nz_gflops': n * g.get_chain().nz_flops_per_element() / (ms / 1e3) / 1e9}
+                                'nz_gflops': n * g.get_chain().nz_flops_per_element() / (ms / 1e3) / 1e9,
+                                'hbm_gbs': n * g.get_chain().bytes_per_element() / (ms / 1e3) / 1e9}
   return out
 
 

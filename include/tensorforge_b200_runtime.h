@@ -1,0 +1,41 @@
+// Entry points of the native runtime library libtfb200_runtime.so (built from
+// tensorforge_b200/csrc/*.cu). None of them has a counterpart in the reference, which has
+// no autotuner and records no rooflines: they back the learned cost model of the
+// autotuner and the measured roofline denominators.
+//
+// Every function is asynchronous on `stream` (a cudaStream_t; nullptr = legacy default
+// stream), allocates nothing, and returns the cudaError_t of its launch (0 = success).
+#pragma once
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+// ---- throughput probes (roofline denominators)
+// 16 independent FMA chains per thread, 256 threads per block, `iters` iterations;
+// flops = 2 * 16 * iters * blocks * 256. `out` holds `blocks` values of the probe's type.
+int tfb_fma_peak_launch(int is_double, void *out, int iters, int blocks, void *stream);
+// 8 independent m8n8k4 FP64 MMA chains per warp, 8 warps per block, `iters` iterations;
+// flops = 512 * 8 * iters * blocks * 8. `out` holds `blocks` doubles.
+int tfb_dmma_peak_launch(void *out, int iters, int blocks, void *stream);
+
+// ---- cost-model MLP, 32 -> 64 -> 64 -> 1 with ReLU, FP32
+// Parameter vector (tfb_mlp_num_params() floats): W1[64][32], b1[64], W2[64][64], b2[64],
+// W3[64], b3. Batches are row-major X[B][32]; T[B] are targets (log runtime).
+int tfb_mlp_num_params(void);
+// Y[B] = MLP(X); H1, H2 ([B][64] each) receive the hidden activations unless nullptr.
+int tfb_mlp_forward(const float *params, const float *X, int B, float *H1, float *H2, float *Y, void *stream);
+// Gradient of L = 1/(2B) sum (Y - T)^2 into grads (overwritten), from the activations of
+// tfb_mlp_forward; dH1, dH2 ([B][64]) and dY ([B]) are scratch.
+int tfb_mlp_backward(const float *params, const float *X, const float *T, int B, const float *H1,
+                     const float *H2, const float *Y, float *dH1, float *dH2, float *dY, float *grads,
+                     void *stream);
+// out[0] = 1/(2B) sum (Y - T)^2
+int tfb_mlp_loss(const float *Y, const float *T, int B, float *out, void *stream);
+// One Adam step (bias-corrected with `step` >= 1) on n parameters; m, v are the moments.
+int tfb_mlp_adam(float *params, const float *grads, float *m, float *v, int n, float lr, float b1, float b2,
+                 float eps, int step, void *stream);
+
+#ifdef __cplusplus
+}
+#endif

@@ -71,7 +71,11 @@ def emit(chain, plan, context, base_name, proto, globals_):
     from .colprog import emit_colprog
     kernel, launch, extra = emit_colprog(chain, plan, context, base_name, globals_)
     return Emitted(kernel, emit_launcher(proto, launch), extra)
-  if plan.strategy in ('tcsplit', 'dmma'):
+  if plan.strategy == 'dmma':
+    from .dmma import emit_dmma
+    kernel, launch, extra = emit_dmma(chain, plan, context, base_name, globals_)
+    return Emitted(kernel, emit_launcher(proto, launch), extra)
+  if plan.strategy == 'tcsplit':
     from .tcsplit import emit_tcsplit
     kernel, launch, extra = emit_tcsplit(chain, plan, context, base_name, globals_)
     return Emitted(kernel, emit_launcher(proto, launch), extra)

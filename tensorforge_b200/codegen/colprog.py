@@ -127,7 +127,8 @@ class _ColProg:
       self.a_base.append(total)
       total += t.A.storage_size()
     self.a_total = total
-    self.ubuf_vals = max(self.TC * self.pitch, self.TC * s.M)
+    # rounded to whole vectors: the staged R copies behind it are read as float4 / double2
+    self.ubuf_vals = _pad(max(self.TC * self.pitch, self.TC * s.M), self.VEC)
     # per-tile copies of the batched R operands (read as 128-bit broadcast loads)
     self.r_off = {}
     r_vals = 0

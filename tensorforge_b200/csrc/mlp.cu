@@ -5,6 +5,7 @@
 // W3[64], b3[1] (row-major, y = W x + b). Batches are row-major [B][features]. Scratch
 // buffers (activations, per-sample deltas) are passed in by the caller.
 #include <cuda_runtime.h>
+#include "tensorforge_b200_runtime.h"
 
 #define TFB_MLP_IN 32
 #define TFB_MLP_H 64

@@ -187,12 +187,28 @@ class Generator:
     from ..plan import make_plan
     from ..codegen import emit
     self._chain = lower(self.descr_list, self._matrix_list, self._globals, self._context.fp_type)
-    self._plan = make_plan(self._chain, self._context)
+    self._plan = make_plan(self._chain, self._context, self._tuned_variant())
     self._emitted = emit(self._chain, self._plan, self._context, self._base_kernel_name,
                          self._generate_launcher_proto(with_defaults=False), self._globals)
     self._kernel = self._emitted.kernel
     self._launcher = self._emitted.launcher
     self._header = f'extern "C" {self._generate_launcher_proto(with_defaults=True)};\n'
+
+  def _tuned_variant(self):
+    """Variant picked by Options.tuner ('model' / 'exhaustive'), None for the planner's own.
+
+    Only plain-precision chains without an explicit variant are tuned; the cost model was
+    trained on FP32 timings, so FP64 chains keep the planner's choice under 'model'.
+    """
+    opts = self._context.get_user_options()
+    if opts.tuner == 'heuristic' or opts.variant or opts.precision != 'plain':
+      return None
+    from ..tune import select
+    if opts.tuner == 'model':
+      if self._context.fp_type.size() != 4:
+        return None
+      return select.model_choice(self._chain, 4)
+    return select.exhaustive_choice(self.descr_list, self._context)
 
   def get_kernel(self):
     return self._kernel

@@ -19,6 +19,8 @@ EXTRA = [
   ('chain_o4_q27', 'float', {'precision': 'tf32x3'}),
   ('chain_o6', 'double', {}),
   ('chain_o6', 'double', {'precision': 'dmma'}),
+  ('chain_o4_q27', 'double', {'precision': 'dmma'}),
+  ('chain_o3_dense', 'double', {'precision': 'dmma'}),
   ('c0_gemm_ptr', 'float', {}),
 ]
 

@@ -50,10 +50,11 @@ def generic_plan(chain, fp_size, threads_per_element=None, elements_per_block=No
   return Plan('generic', {'threads_per_element': g, 'elements_per_block': e}, total, g * e)
 
 
-def make_plan(chain, context):
+def make_plan(chain, context, variant=None):
+  """Plan for `chain`; `variant` (a tuner's pick) overrides Options.variant."""
   opts = context.get_user_options()
   fp_size = context.fp_type.size()
-  variant = opts.variant or {}
+  variant = variant or opts.variant or {}
   forced = variant.get('strategy')
   precision = opts.precision
   from . import chains as chainplan

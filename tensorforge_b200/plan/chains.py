@@ -193,4 +193,5 @@ def tcsplit_plan(chain, shape, precision, variant):
 
 
 def dmma_plan(chain, shape, variant):
-  return None
+  from ..codegen import dmma
+  return dmma.plan(chain, shape, variant, SMEM_LIMIT)

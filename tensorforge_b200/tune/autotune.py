@@ -92,14 +92,18 @@ def buffer_sizes(generator, batch):
   return out, dest
 
 
-def build_chain(spec, extra_flags=()):
-  """Generate and compile all variants of `spec` (host only; safe in a worker process)."""
+def build_chain(spec, extra_flags=(), compile=True):
+  """Generate and compile all variants of `spec` (host only; safe in a worker process).
+
+  With compile=False only the record is made (so_path None): for chains whose timings are
+  already cached.
+  """
   src, gens, default = variant_library(spec)
-  so = build_library(src, extra_flags)
+  so = build_library(src, extra_flags) if compile else None
   g0 = gens[0][1]
   return ChainBuild(spec, so, g0.abi_params(), *buffer_sizes(g0, spec.batch),
                     [g.get_base_name() for _, g in gens], [v for v, _ in gens],
-                    [features(spec, gens[0][1].get_chain(), v) for v, g in gens], default)
+                    [features(gens[0][1].get_chain(), v, spec.batch) for v, g in gens], default)
 
 
 class _Abi:
@@ -129,6 +133,10 @@ def gpu_signature():
   except Exception:  # NVML missing: key on the device name alone
     drv = 'unknown'
   return f'{torch.cuda.get_device_name()}_drv{drv}'.replace(' ', '_')
+
+
+def is_cached(cache, spec, gpu):
+  return os.path.exists(_cache_path(cache, spec, gpu))
 
 
 def _cache_path(cache, spec, gpu):

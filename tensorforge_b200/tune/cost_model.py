@@ -133,6 +133,23 @@ class CostModel:
     self.mean, self.std = z['mean'], z['std']
 
 
+def host_predict(params, mean, std, feats):
+  """Predicted log-runtime on the host (numpy), for picking a variant at generation time,
+  where no GPU need be present. Same parameter layout and arithmetic as tfb_mlp_forward."""
+  p = np.asarray(params, np.float64)
+  o = 0
+  W1 = p[o:o + HID * NFEAT].reshape(HID, NFEAT); o += HID * NFEAT
+  b1 = p[o:o + HID]; o += HID
+  W2 = p[o:o + HID * HID].reshape(HID, HID); o += HID * HID
+  b2 = p[o:o + HID]; o += HID
+  W3 = p[o:o + HID]; o += HID
+  b3 = p[o]
+  X = (np.asarray(feats, np.float64) - mean) / std
+  h1 = np.maximum(X @ W1.T + b1, 0.0)
+  h2 = np.maximum(h1 @ W2.T + b2, 0.0)
+  return h2 @ W3 + b3
+
+
 def top_k(pred_log_ms, k=5):
   return list(np.argsort(pred_log_ms)[:k])
 

@@ -3,12 +3,13 @@ cost model on a held-out split.
 
     python -m tensorforge_b200.tune.run --chains 2000 --jobs 32 --time-limit 1800 --out DIR
 
-Chain libraries are compiled by a pool of `--jobs` spawned worker processes (started
-before CUDA is initialised) while this process measures finished libraries on the GPU, in
-chain order, until `--time-limit` seconds have passed. Per-chain timings are cached in
-DIR/cache (a rerun with the same DIR resumes). Chains are split by a multiplicative hash of their index
-into training (80 %) and test sets; the cost model is trained on the training chains by the
-CUDA MLP kernels and scored on the test chains:
+Chain libraries are compiled by a pool of `--jobs` worker processes (spawn start method, so
+they never inherit this process's CUDA context) while this process measures finished
+libraries on the GPU, in chain order, until `--time-limit` seconds have passed. Per-chain
+timings are cached in DIR/cache; a rerun with the same DIR resumes and does not compile the
+cached chains again. Chains are split by a multiplicative hash of their index into training
+(80 %) and test sets; the cost model is trained on the training chains by the CUDA MLP
+kernels and scored on the test chains:
 
   regret(pick) = (measured time of pick - exhaustive best) / exhaustive best
 
@@ -26,12 +27,12 @@ import time
 import numpy as np
 
 
-def _build(spec, kcache):
+def _build(spec, kcache, compile=True):
   if kcache:
     os.environ['TFB_KCACHE'] = kcache
   from .autotune import build_chain
   t = time.time()
-  cb = build_chain(spec)
+  cb = build_chain(spec, compile=compile)
   return cb, time.time() - t
 
 
@@ -42,12 +43,15 @@ def is_test_chain(index):
 
 def collect(specs, jobs, time_limit, out, kcache=None, keep_libs=False, log=print):
   """Build (pool) and measure (this process) chains; returns the measured records."""
-  from .autotune import measure_chain
+  from .autotune import measure_chain, is_cached, gpu_signature
   t0 = time.time()
   ctx = mp.get_context('spawn')
   records = []
+  cache = os.path.join(out, 'cache')
+  sig = gpu_signature()
   pool = cf.ProcessPoolExecutor(max_workers=jobs, mp_context=ctx)
-  futs = [pool.submit(_build, s, kcache) for s in specs]
+  # chains with cached timings are not compiled again (their records are still generated)
+  futs = [pool.submit(_build, s, kcache, not is_cached(cache, s, sig)) for s in specs]
   build_s = []
   try:
     for i, f in enumerate(futs):
@@ -61,14 +65,15 @@ def collect(specs, jobs, time_limit, out, kcache=None, keep_libs=False, log=prin
       except Exception as e:  # a chain that does not generate or compile is reported and skipped
         log(f'chain {specs[i].index}: build failed: {str(e).splitlines()[0][:200]}')
         continue
-      build_s.append(bt)
+      if cb.so_path is not None:
+        build_s.append(bt)
       try:
-        res = measure_chain(cb, cache=os.path.join(out, 'cache'))
+        res = measure_chain(cb, cache=cache)
       except Exception as e:  # the planner default itself failed to launch
         log(f'chain {specs[i].index}: measurement failed: {str(e).splitlines()[0][:200]}')
         continue
       records.append((cb, res))
-      if not keep_libs and kcache:
+      if not keep_libs and kcache and cb.so_path is not None:
         try:
           os.remove(cb.so_path)
         except OSError:

@@ -1,0 +1,89 @@
+"""Variant selection at generation time: `Options(tuner='model')` and `tuner='exhaustive'`.
+
+'model'       ranks every applicable variant with the trained cost model (weights shipped
+              in model_b200.npz, trained on B200 timings; evaluated on the host, no GPU
+              needed) and takes the best predicted one.
+'exhaustive'  builds every variant and times it on the current GPU (CUDA events, best of
+              3) with synthetic inputs of `batch` elements, and takes the fastest.
+
+Both only choose among variants of the plain-precision generators (generic and column
+programs); the tensor-core precisions have one plan each. Launchers are generic in
+numElements, so the batch the choice is made for is a parameter (default 100,000).
+"""
+import os
+
+import numpy as np
+
+from .variants import variant_space, features
+
+DEFAULT_BATCH = 100_000
+MODEL_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'model_b200.npz')
+_model = None
+
+
+def _load_model():
+  global _model
+  if _model is None:
+    if not os.path.exists(MODEL_PATH):
+      raise FileNotFoundError(f'cost model weights missing: {MODEL_PATH}')
+    z = np.load(MODEL_PATH)
+    _model = (z['params'], z['mean'], z['std'])
+  return _model
+
+
+def model_choice(chain, fp_size=4, batch=DEFAULT_BATCH):
+  """Variant dict with the lowest predicted runtime, or None if there is no choice."""
+  from .cost_model import host_predict
+  cands = variant_space(chain, fp_size)
+  if len(cands) < 2:
+    return None
+  params, mean, std = _load_model()
+  pred = host_predict(params, mean, std, [features(chain, v, batch) for v in cands])
+  return cands[int(np.argmin(pred))]
+
+
+def exhaustive_choice(descr_list, context, batch=DEFAULT_BATCH, reps=3):
+  """Build and time every variant of `descr_list` on the current GPU; the fastest wins."""
+  import torch
+  from ..common.context import Context, Options
+  from ..generators.generator import Generator
+  from ..runtime.kernel import CompiledKernel
+  opts = context.get_user_options()
+
+  def gen(variant):
+    o = Options(opts.exact_contraction_length, opts.align_shr_mem, opts.enable_sync_block_opt,
+                opts.precision, 'heuristic', variant)
+    g = Generator(descr_list, Context(context.arch, context.backend, context.fp_type, o))
+    g.generate()
+    return g
+
+  base = gen(None)
+  cands = variant_space(base.get_chain(), context.fp_type.size())
+  if len(cands) < 2:
+    return None
+  dtype = torch.float64 if context.fp_type.size() == 8 else torch.float32
+  bufs = {}
+  for t, _ in base.abi_symbols():
+    if t.addressing.name == 'SCALAR':
+      continue
+    if t.addressing.name == 'PTR_BASED':
+      return None  # pointer arrays would need per-element buffers: keep the heuristic plan
+    size = t.spp.count_nz() if t.addressing.name == 'NONE' else batch * t.get_real_volume()
+    bufs[t.name] = torch.rand(max(1, size), device='cuda', dtype=dtype)
+  scalars = {t.name: 1.0 for t, _ in base.abi_symbols() if t.addressing.name == 'SCALAR'}
+  stream = torch.cuda.current_stream()
+  best, best_ms = None, float('inf')
+  for v in cands:
+    k = CompiledKernel(gen(v))
+    kw = dict(bufs, **scalars)
+    k(numElements=batch, **kw)
+    for _ in range(reps):
+      s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+      s.record(stream)
+      k(numElements=batch, **kw)
+      e.record(stream)
+      e.synchronize()
+      ms = s.elapsed_time(e)
+      if ms < best_ms:
+        best, best_ms = v, ms
+  return best

@@ -38,16 +38,25 @@ def _l2(x):
   return math.log2(max(1.0, float(x)))
 
 
-def chain_features(spec, chain):
-  """20 features of the chain itself."""
-  f = [len(spec.stages) / 4.0]
+def _stage_density(stage):
+  """Density of the stage's stored (non-temporary) operands: the sparsest one's."""
+  d = [r.op.tensor.density() for r in stage.ops if r.op.kind != 'tmp' and r.op.sparse]
+  return min(d) if d else 1.0
+
+
+def chain_features(chain, batch):
+  """20 features of the lowered chain and its batch size (up to 4 stages described)."""
+  st = chain.stages
+  f = [len(st) / 4.0]
   for i in range(4):
-    if i < len(spec.stages):
-      s = spec.stages[i]
-      f += [_l2(s.rows) / 7.0, _l2(s.cols) / 7.0, _l2(s.k) / 7.0, s.density]
+    if i < len(st):
+      s = st[i]
+      rows = s.n_ranges[0][1] - s.n_ranges[0][0] if s.n_ranges else 1
+      cols = s.n_ranges[1][1] - s.n_ranges[1][0] if len(s.n_ranges) > 1 else 1
+      f += [_l2(rows) / 7.0, _l2(cols) / 7.0, _l2(s.k_volume()) / 7.0, _stage_density(s)]
     else:
       f += [0.0, 0.0, 0.0, 0.0]
-  f.append(math.log10(spec.batch) / 6.0)
+  f.append(math.log10(max(1, batch)) / 6.0)
   f.append(math.log10(max(1.0, chain.nz_flops_per_element())) / 7.0)
   f.append(math.log10(max(1.0, chain.bytes_per_element())) / 6.0)
   return f
@@ -74,11 +83,12 @@ def variant_features(chain, variant, fp_size=4):
           te * shape.N / t, 0.0, 0.0, shape.M / 128.0, len(shape.terms) / 4.0, 0.0]
 
 
-def features(spec, chain, variant):
-  cf = getattr(chain, '_tune_features', None)
-  if cf is None:  # the chain part is shared by all variants (and costs a nonzero count)
-    cf = chain._tune_features = chain_features(spec, chain)
-  f = cf + variant_features(chain, variant)
+def features(chain, variant, batch):
+  """The cost model's input for running `variant` of `chain` on `batch` elements."""
+  memo = chain.__dict__.setdefault('_tune_features', {})
+  if batch not in memo:  # the chain part is shared by all variants (and costs a nonzero count)
+    memo[batch] = chain_features(chain, batch)
+  f = memo[batch] + variant_features(chain, variant)
   assert len(f) == NFEAT, len(f)
   return f
 

@@ -69,7 +69,8 @@ def test_fit_learns_a_smooth_function():
   hist = m.fit(X[:3000], y[:3000], steps=1500, lr=3e-3, batch=1024)
   assert hist[-1][1] < 0.1 * hist[0][1]
   pred = m.predict(X[3000:])
-  assert np.sqrt(np.mean((pred - y[3000:]) ** 2)) < 0.25
+  # held-out error well below the target's spread (28 of the 32 inputs are noise)
+  assert np.sqrt(np.mean((pred - y[3000:]) ** 2)) < 0.5 * np.std(y[3000:])
 
 
 def test_tuning_run_measures_consistent_variants(tmp_path):

@@ -58,7 +58,7 @@ def test_features_shape_and_finite():
   for spec in random_chains(20, seed=5, hi=32):
     base = autotune.make_generator(spec)
     for v in variants.variant_space(base.get_chain()):
-      f = variants.features(spec, base.get_chain(), v)
+      f = variants.features(base.get_chain(), v, spec.batch)
       assert len(f) == variants.NFEAT
       assert all(math.isfinite(x) for x in f)
 
