@@ -8,8 +8,8 @@ one MMA chain per tile of TE = floor(128 / N) whole elements (TE*N flat output c
   * M = 128 rows = flat columns (e, j) (one TMEM lane each), N = rows of out padded to 16,
     K = sum_t K_t (each term padded to the MMA K step);
   * A operand (U^T, per element) lives in tensor memory. Per tile, the batched operands
-    are prefetched one tile ahead into a double-buffered shared-memory stage with
-    cp.async (coalesced 16-byte chunks); one producer thread per (element, row l)
+    are fetched one tile ahead into a shared-memory stage (see the pipelines below); one
+    producer thread per (element, row l)
     computes row l of U_t = B_e * R_{e,t} for all j with R_t's compile-time pattern
     unrolled and writes it to a padded transposition buffer; then each lane reads its
     column (e, j), splits it into hi + lo and writes both with tcgen05.st;
@@ -36,6 +36,20 @@ the tensor cores work on tile n while the producers compute tile n+1; tile n's e
 then frees the accumulators for tile n+1. Every mbarrier wait is bounded: on timeout the
 kernel records an error code (read with tfb_kernel_error_<name>) and exits after
 releasing its tensor memory.
+
+Producer pipelines (plan option `pipe`):
+  2 (default when it fits in shared memory): one input stage, filled by one bulk copy
+    (cp.async.bulk global -> shared, no multicast) per contiguous, 16-byte aligned B block
+    and cp.async for the R blocks, completion tracked by a stage mbarrier (expect_tx bytes
+    plus one cp.async arrival per producer); one U pass computes U_t for every term (B's
+    row loaded once) into one transposition buffer per term; the previous tile's output
+    is staged over the consumed B block and written with one bulk store. Three named
+    barriers per tile.
+  1: the original per-term pipeline (double-buffered cp.async stage, U phase and lane
+    phase per term, two transposition buffers); used when pipe 2 does not fit.
+The bulk B copy is issued by producer 0 after its output bulk store has read the stage;
+when a B block is not contiguous or not 16-byte aligned, every producer copies it with
+cp.async after one more barrier.
 """
 from .. import plan as _plan
 from ..plan import Plan
@@ -95,6 +109,43 @@ def smem_plan(shape, precision):
               ubuf_bytes=_pad(ubuf, 128), off_bar=off_bar, total=total, te=te, tc=tc)
 
 
+def _bulk_eligible(op, vals):
+  """A tile of this operand is one contiguous block: one bulk copy when aligned at run time."""
+  return op.addressing.name == 'STRIDED' and op.element_volume() == vals and (vals * 4) % 16 == 0
+
+
+def smem_plan_v2(shape, precision):
+  """Shared memory of the one-pass pipeline: single input stage (B blocks first, the tile's
+  output staged over them, R blocks behind both) and one transposition buffer per term."""
+  lay = layout(shape, precision)
+  te = lay['te']
+  tc = te * shape.N
+  b_ops = []
+  for t in shape.terms:
+    if all(t.B is not o for o in b_ops):
+      b_ops.append(t.B)
+  r_ops = [op for op, _ in staged_operands(shape) if all(op is not o for o in b_ops)]
+  stage_off = {}
+  off = 0
+  for op in b_ops:
+    stage_off[op.name] = off
+    off += te * _pad(op.element_volume(), 4)
+  off = _pad(max(off, te * shape.out.element_volume()), 4)
+  for op in r_ops:
+    stage_off[op.name] = off
+    off += te * _pad(op.storage_size() if op.sparse else op.element_volume(), 4)
+  stage = _pad(off * 4, 128)
+  kmax = max(t.K for t in shape.terms)
+  pitch = _pad(kmax, 4) + 4
+  ubuf = _pad(tc * pitch * 4, 128)
+  off_stage = _pad(lay['b_bytes'], 128)
+  off_u = off_stage + stage
+  off_bar = off_u + len(shape.terms) * ubuf
+  total = off_bar + 256
+  return dict(off_stage=off_stage, stage=stage, stage_off=stage_off, b_ops=b_ops, r_ops=r_ops, off_u=off_u,
+              pitch=pitch, ubuf_bytes=ubuf, off_bar=off_bar, total=total, te=te, tc=tc)
+
+
 def plan(chain, shape, precision, variant):
   if precision not in KSTEP:
     return None
@@ -106,12 +157,16 @@ def plan(chain, shape, precision, variant):
   for t in shape.terms:
     if t.R is not None and t.R.kind != 'batched':
       return None
-  sm = smem_plan(shape, precision)
+  pipe = variant.get('pipe', 2)
+  sm = smem_plan_v2(shape, precision) if pipe == 2 else None
+  if sm is None or sm['total'] > _plan.SMEM_LIMIT:
+    pipe = 1
+    sm = smem_plan(shape, precision)
   smem = max(sm['total'], 120 * 1024)  # one CTA per SM: it owns the SM's tensor memory
   if smem > _plan.SMEM_LIMIT:
     return None
   chunk = variant.get('chunk', 16)
-  return Plan('tcsplit', {'precision': precision, 'chunk': chunk}, smem, 32 * (4 * H_GROUPS + 1),
+  return Plan('tcsplit', {'precision': precision, 'chunk': chunk, 'pipe': pipe}, smem, 32 * (4 * H_GROUPS + 1),
               note=f'M={shape.M} N={shape.N} terms={len(shape.terms)} tmem={lay["tmem_used"]} smem={sm["total"]}')
 
 
@@ -215,6 +270,19 @@ __device__ __forceinline__ void bulk_store(void* gdst, const void* ssrc, unsigne
                :: "l"(gdst), "r"(smem_u32(ssrc)), "r"(bytes) : "memory");
   asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 }
+// global -> shared bulk copy (no multicast), completion counted in bytes on `bar`
+__device__ __forceinline__ void bulk_load(void* sdst, const void* gsrc, unsigned bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               :: "r"(smem_u32(sdst)), "l"(gsrc), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}"
+               :: "r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// arrive on `bar` once this thread's earlier cp.async copies have landed (counts as an arrival)
+__device__ __forceinline__ void cp_async_mbar_arrive(uint64_t* bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" :: "r"(smem_u32(bar)) : "memory");
+}
 __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 }  // namespace tfb_tc
@@ -238,7 +306,8 @@ class _TC:
     self.base = base
     self.prec = plan_.params['precision']
     self.lay = layout(shape, self.prec)
-    self.sm = smem_plan(shape, self.prec)
+    self.pipe = plan_.params.get('pipe', 1)
+    self.sm = smem_plan_v2(shape, self.prec) if self.pipe == 2 else smem_plan(shape, self.prec)
     self.LC = plan_.params['chunk']
     self.H = H_GROUPS
     self.lines = []
@@ -294,6 +363,8 @@ class _TC:
     for op, vals in staged:
       stage_off[op.name] = off          # floats, within one stage buffer
       off += te * _pad(vals, 4)
+    if self.pipe == 2:
+      stage_off = dict(sm['stage_off'])
     # B operand blocks (hi/lo per term) at the start of shared memory
     ke = 16 // es
     b_off = []
@@ -351,11 +422,18 @@ class _TC:
     self.ind += 1
     self.w('extern __shared__ __align__(1024) unsigned char tfb_smem_raw[];')
     self.w(f'uint64_t* const bars = reinterpret_cast<uint64_t*>(tfb_smem_raw + {sm["off_bar"]});')
-    self.w(f'unsigned* const tmem_slot = reinterpret_cast<unsigned*>(bars + {2 * nterms + 2});')
-    self.w(f'float* const stage0 = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_stage"]});')
-    self.w(f'float* const stage1 = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_stage"] + sm["stage"]});')
-    self.w(f'float* const ubuf0 = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_u"]});')
-    self.w(f'float* const ubuf1 = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_u"] + (sm["ubuf_bytes"] if sm["nbuf"] == 2 else 0)});')
+    nbars = 2 * nterms + (3 if self.pipe == 2 else 2)
+    BAR_STAGE = 2 * nterms + 2
+    self.w(f'unsigned* const tmem_slot = reinterpret_cast<unsigned*>(bars + {nbars});')
+    if self.pipe == 2:
+      self.w(f'float* const stage = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_stage"]});')
+      for ti in range(nterms):
+        self.w(f'float* const ubuf{ti} = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_u"] + ti * sm["ubuf_bytes"]});')
+    else:
+      self.w(f'float* const stage0 = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_stage"]});')
+      self.w(f'float* const stage1 = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_stage"] + sm["stage"]});')
+      self.w(f'float* const ubuf0 = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_u"]});')
+      self.w(f'float* const ubuf1 = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_u"] + (sm["ubuf_bytes"] if sm["nbuf"] == 2 else 0)});')
     self.w('const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;')
     self.w(f'const size_t numTiles = (numElements + {te - 1}u) / {te}u;')
     # ---- setup: B operand, barriers, TMEM
@@ -385,6 +463,9 @@ class _TC:
       self.w(f'tfb_tc::mbar_init(&bars[{BAR_FREE + ti}], 1u);')
     self.w(f'tfb_tc::mbar_init(&bars[{BAR_DFULL}], 1u);')
     self.w(f'tfb_tc::mbar_init(&bars[{BAR_DFREE}], {NP}u);')
+    if self.pipe == 2:
+      # one arrival per producer (cp.async completion) + the bulk-copy issuer's expect_tx
+      self.w(f'tfb_tc::mbar_init(&bars[{BAR_STAGE}], {NP + 1}u);')
     self.w('asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");')
     self.close()
     self.open('if (warp == 0)')
@@ -428,52 +509,55 @@ class _TC:
     self.close()
     self.close()
     # ---- producers
-    self.open(f'else if (warp < {4 * H})')
-    self.w('const unsigned ptid = threadIdx.x;')
-    self.w('const unsigned quad = warp & 3u, grp = warp >> 2;')
-    self.w('const unsigned row = quad * 32u + lane;')
-    self.w('const unsigned lane_addr = tmem + ((quad * 32u) << 16);')
-    self.w(f'const bool lane_col = row < {tcols}u;')
-    self.w(f'const unsigned le = row / {s.N}u, lj = row - le * {s.N}u;')
-    self.w('unsigned it = 0;')
-    self.w('size_t prev_tile = 0; bool have_prev = false;')
-    self.open('if (blockIdx.x < numTiles)')
-    self._prefetch('(size_t)blockIdx.x', 'stage0')
-    self.close()
-    self.w('tfb_tc::cp_async_commit();')
-    self.open('for (size_t tile = blockIdx.x; ; tile += gridDim.x, ++it)')
-    self.w('// every producer takes the same branches around named barriers: a timeout anywhere')
-    self.w('// stops all producers at the next tile boundary (a barrier-wide OR), never mid-tile')
-    self.w(f'if (tfb_tc::any_sync(1, {NP}, !ok)) break;')
-    self.w('const bool more = tile < numTiles;')
-    self.w('float* const cur = (it & 1u) ? stage1 : stage0;')
-    self.w('float* const nxt = (it & 1u) ? stage0 : stage1;')
-    self.open('if (more)')
-    self.w('const size_t ntile = tile + gridDim.x;')
-    self.open('if (ntile < numTiles)')
-    self._prefetch('ntile', 'nxt')
-    self.close()
-    self.w('tfb_tc::cp_async_commit();')
-    self.w('tfb_tc::cp_async_wait_one();')
-    self.w(f'tfb_tc::named_sync(1, {NP});')
-    self.w(f'const size_t e0 = tile * {te}u;')
-    self.w('const size_t el = e0 + le;')
-    self.w('const bool active = lane_col && el < numElements && (flags == nullptr || flags[el] != 0u);')
-    for ti, t in enumerate(s.terms):
-      self._term(ti, t, slot_base[ti], stage_off, lim, NP)
-    self.close()
-    # epilogue of the previous tile
-    self.open('if (have_prev)')
-    self.w(f'if (!tfb_tc::mbar_wait(&bars[{BAR_DFULL}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 20u); }}')
-    self.w('tfb_tc::fence_after();')
-    self._epilogue(d_main, d_corr, NP)
-    self.close()
-    self.w('if (!more) break;')
-    self.w('prev_tile = tile; have_prev = true;')
-    self.close()
-    self.w('tfb_tc::cp_async_wait_all();')
-    self.w('if (ptid == 0) tfb_tc::bulk_wait();')
-    self.close()
+    if self.pipe == 2:
+      self._producers_v2(s, te, tcols, NP, stage_off, slot_base, lim, BAR_DFULL, BAR_STAGE, d_main, d_corr)
+    else:
+      self.open(f'else if (warp < {4 * H})')
+      self.w('const unsigned ptid = threadIdx.x;')
+      self.w('const unsigned quad = warp & 3u, grp = warp >> 2;')
+      self.w('const unsigned row = quad * 32u + lane;')
+      self.w('const unsigned lane_addr = tmem + ((quad * 32u) << 16);')
+      self.w(f'const bool lane_col = row < {tcols}u;')
+      self.w(f'const unsigned le = row / {s.N}u, lj = row - le * {s.N}u;')
+      self.w('unsigned it = 0;')
+      self.w('size_t prev_tile = 0; bool have_prev = false;')
+      self.open('if (blockIdx.x < numTiles)')
+      self._prefetch('(size_t)blockIdx.x', 'stage0')
+      self.close()
+      self.w('tfb_tc::cp_async_commit();')
+      self.open('for (size_t tile = blockIdx.x; ; tile += gridDim.x, ++it)')
+      self.w('// every producer takes the same branches around named barriers: a timeout anywhere')
+      self.w('// stops all producers at the next tile boundary (a barrier-wide OR), never mid-tile')
+      self.w(f'if (tfb_tc::any_sync(1, {NP}, !ok)) break;')
+      self.w('const bool more = tile < numTiles;')
+      self.w('float* const cur = (it & 1u) ? stage1 : stage0;')
+      self.w('float* const nxt = (it & 1u) ? stage0 : stage1;')
+      self.open('if (more)')
+      self.w('const size_t ntile = tile + gridDim.x;')
+      self.open('if (ntile < numTiles)')
+      self._prefetch('ntile', 'nxt')
+      self.close()
+      self.w('tfb_tc::cp_async_commit();')
+      self.w('tfb_tc::cp_async_wait_one();')
+      self.w(f'tfb_tc::named_sync(1, {NP});')
+      self.w(f'const size_t e0 = tile * {te}u;')
+      self.w('const size_t el = e0 + le;')
+      self.w('const bool active = lane_col && el < numElements && (flags == nullptr || flags[el] != 0u);')
+      for ti, t in enumerate(s.terms):
+        self._term(ti, t, slot_base[ti], stage_off, lim, NP)
+      self.close()
+      # epilogue of the previous tile
+      self.open('if (have_prev)')
+      self.w(f'if (!tfb_tc::mbar_wait(&bars[{BAR_DFULL}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 20u); }}')
+      self.w('tfb_tc::fence_after();')
+      self._epilogue(d_main, d_corr, NP)
+      self.close()
+      self.w('if (!more) break;')
+      self.w('prev_tile = tile; have_prev = true;')
+      self.close()
+      self.w('tfb_tc::cp_async_wait_all();')
+      self.w('if (ptid == 0) tfb_tc::bulk_wait();')
+      self.close()
     # ---- teardown
     self.w('tfb_tc::fence_before();')
     self.w('__syncthreads();')
@@ -529,6 +613,174 @@ class _TC:
       self.close()
       off += te * vp
 
+  # ------------------------------------------------------------------ one-pass pipeline
+  def _cp_async_copy(self, op, vals, off, tile_expr, buf, NP):
+    """cp.async one operand's values of a tile into `buf` + off (16-byte chunks when aligned)."""
+    te = self.sm['te']
+    vp = _pad(vals, 4)
+    self.open('')
+    self.w(f'const size_t pe0 = ({tile_expr}) * {te}u;')
+    if vals % 4 == 0:
+      self.open(f'for (unsigned q = ptid; q < {te * vals // 4}u; q += {NP}u)')
+      self.w(f'const unsigned ei = q / {vals // 4}u, c4 = q - ei * {vals // 4}u;')
+      self.w('const size_t ee = pe0 + ei;')
+      self.open('if (ee < numElements)')
+      self.w(f'const float* src = {self._elem_ptr(op, "ee")} + 4u * c4;')
+      self.w(f'float* dst = {buf} + {off} + ei * {vp}u + 4u * c4;')
+      self.w('if ((reinterpret_cast<uintptr_t>(src) & 15u) == 0u) tfb_tc::cp_async16(dst, src);')
+      self.w('else { tfb_tc::cp_async4(dst, src); tfb_tc::cp_async4(dst + 1, src + 1); '
+             'tfb_tc::cp_async4(dst + 2, src + 2); tfb_tc::cp_async4(dst + 3, src + 3); }')
+      self.close()
+      self.close()
+    else:
+      self.open(f'for (unsigned q = ptid; q < {te * vals}u; q += {NP}u)')
+      self.w(f'const unsigned ei = q / {vals}u, c = q - ei * {vals}u;')
+      self.w('const size_t ee = pe0 + ei;')
+      self.w(f'if (ee < numElements) tfb_tc::cp_async4({buf} + {off} + ei * {vp}u + c, {self._elem_ptr(op, "ee")} + c);')
+      self.close()
+    self.close()
+
+  def _loads_v2(self, tile_expr, part, stage_off, BAR_STAGE, NP):
+    """Inputs of tile `tile_expr` into the stage. part 1: the R blocks (cp.async by every
+    producer; their region never overlaps the staged output). part 2: the B blocks, one
+    bulk copy each when every block is contiguous and 16-byte aligned (issued by producer 0
+    after its output bulk store has read the stage), else cp.async by every producer after
+    a barrier; then every producer arrives on the stage barrier once its copies land."""
+    sm = self.sm
+    te = sm['te']
+    if part == 1:
+      for op in sm['r_ops']:
+        vals = op.storage_size() if op.sparse else op.element_volume()
+        self._cp_async_copy(op, vals, stage_off[op.name], tile_expr, 'stage', NP)
+      return
+    b_ops = sm['b_ops']
+    eligible = all(_bulk_eligible(op, op.element_volume()) for op in b_ops)
+    self.open('')
+    self.w(f'const size_t be0 = ({tile_expr}) * {te}u;')
+    self.w(f'const unsigned bnv = (unsigned)((numElements - be0) < {te}u ? (numElements - be0) : {te}u);')
+    if eligible:
+      conds = ' && '.join(f'((reinterpret_cast<uintptr_t>({op.name} + be0 * {op.element_volume()}u + '
+                          f'{op.name}_extraOffset) & 15u) == 0u)' for op in b_ops)
+      self.w(f'const bool bulk_in = {conds};')
+    else:
+      self.w('const bool bulk_in = false;')
+    per_elem = sum(op.element_volume() * 4 for op in b_ops)
+    self.open('if (bulk_in)')
+    self.open('if (ptid == 0)')
+    self.w(f'tfb_tc::mbar_arrive_expect_tx(&bars[{BAR_STAGE}], bnv * {per_elem}u);')
+    for op in b_ops:
+      self.w(f'tfb_tc::bulk_load(stage + {stage_off[op.name]}, {op.name} + be0 * {op.element_volume()}u + '
+             f'{op.name}_extraOffset, bnv * {op.element_volume() * 4}u, &bars[{BAR_STAGE}]);')
+    self.close()
+    self.close()
+    self.open('else')
+    self.w(f'tfb_tc::named_sync(1, {NP});  // the previous tile\'s staged output has been read')
+    for op in b_ops:
+      self._cp_async_copy(op, op.element_volume(), stage_off[op.name], tile_expr, 'stage', NP)
+    self.w(f'if (ptid == 0) tfb_tc::mbar_arrive(&bars[{BAR_STAGE}]);')
+    self.close()
+    self.w(f'tfb_tc::cp_async_mbar_arrive(&bars[{BAR_STAGE}]);')
+    self.close()
+
+  def _u_phase_v2(self, stage_off, NP):
+    """U_t = B * R_t for every term in one pass: one thread per (element, row l) loads row l
+    of B once and writes row l of every U_t that uses it (R_t's pattern unrolled)."""
+    s, sm = self.s, self.sm
+    te, pitch, N = sm['te'], sm['pitch'], s.N
+    comp = ['x', 'y', 'z', 'w']
+    for B in sm['b_ops']:
+      terms = [(ti, t) for ti, t in enumerate(s.terms) if t.B is B]
+      K, P = terms[0][1].K, terms[0][1].P
+      bvals = _pad(B.element_volume(), 4)
+      self.open(f'for (unsigned q = ptid; q < {te * K}u; q += {NP}u)')
+      self.w(f'const unsigned ei = q / {K}u, l = q - ei * {K}u;')
+      self.w(f'const float* const bq = stage + {stage_off[B.name]} + ei * {bvals}u + l;')
+      for m in range(P):
+        self.w(f'const float q{m} = bq[{m * K}];')
+      for ti, t in terms:
+        dst = f'ubuf{ti}[(ei * {N}u + {{j}}u) * {pitch}u + l]'
+        if t.R is None:
+          for j in range(N):
+            self.w(f'{dst.format(j=j)} = q{j};')
+          continue
+        nr = t.R.storage_size()
+        self.open('')
+        self.w(f'const float4* const rq = reinterpret_cast<const float4*>(stage + {stage_off[t.R.name]} + ei * {_pad(nr, 4)}u);')
+        for v in range((nr + 3) // 4):
+          self.w(f'const float4 r{v} = rq[{v}];')
+        look = t.R.sparse_lookup() if t.R.sparse else None
+        for j in range(N):
+          expr = '0.0f'
+          for m in range(P):
+            pos = look.get((m, j)) if look is not None else j * P + m
+            if pos is not None:
+              expr = f'fmaf(q{m}, r{pos // 4}.{comp[pos % 4]}, {expr})'
+          self.w(f'{dst.format(j=j)} = {expr};')
+        self.close()
+      self.close()
+
+  def _producers_v2(self, s, te, tcols, NP, stage_off, slot_base, lim, BAR_DFULL, BAR_STAGE, d_main, d_corr):
+    """Producer warps, one-pass pipeline. Per tile: [barrier D: abort OR] wait for the stage,
+    U phase of all terms, [barrier A], R blocks of the next tile, epilogue of the previous
+    tile ([barrier B] + bulk store when staged), B blocks of the next tile, lane phases."""
+    b, H = self.base, self.H
+    pitch = self.sm['pitch']
+    self.open(f'else if (warp < {4 * H})')
+    self.w('const unsigned ptid = threadIdx.x;')
+    self.w('const unsigned quad = warp & 3u, grp = warp >> 2;')
+    self.w('const unsigned row = quad * 32u + lane;')
+    self.w('const unsigned lane_addr = tmem + ((quad * 32u) << 16);')
+    self.w(f'const bool lane_col = row < {tcols}u;')
+    self.w(f'const unsigned le = row / {s.N}u, lj = row - le * {s.N}u;')
+    self.w('unsigned it = 0;')
+    self.w('size_t prev_tile = 0; bool have_prev = false; bool pending = false;')
+    self.open('if (blockIdx.x < numTiles)')
+    self._loads_v2('(size_t)blockIdx.x', 1, stage_off, BAR_STAGE, NP)
+    self._loads_v2('(size_t)blockIdx.x', 2, stage_off, BAR_STAGE, NP)
+    self.w('pending = true;')
+    self.close()
+    self.open('for (size_t tile = blockIdx.x; ; tile += gridDim.x, ++it)')
+    self.w('// every producer takes the same branches around named barriers: a timeout anywhere')
+    self.w('// stops all producers at the next tile boundary (a barrier-wide OR), never mid-tile')
+    self.w(f'if (tfb_tc::any_sync(1, {NP}, !ok)) break;')
+    self.w('const bool more = tile < numTiles;')
+    self.w('const size_t ntile = tile + gridDim.x;')
+    self.w('const bool has_next = more && ntile < numTiles;')
+    self.open('if (more)')
+    self.w(f'if (!tfb_tc::mbar_wait(&bars[{BAR_STAGE}], it & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 40u); }}')
+    self.w('pending = false;')
+    self._u_phase_v2(stage_off, NP)
+    self.close()
+    self.w(f'tfb_tc::named_sync(1, {NP});')
+    self.open('if (has_next)')
+    self._loads_v2('ntile', 1, stage_off, BAR_STAGE, NP)
+    self.close()
+    self.open('if (have_prev)')
+    self.w(f'if (!tfb_tc::mbar_wait(&bars[{BAR_DFULL}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 20u); }}')
+    self.w('tfb_tc::fence_after();')
+    self._epilogue(d_main, d_corr, NP, sbuf='stage', final_sync=False)
+    self.close()
+    self.open('if (has_next)')
+    self._loads_v2('ntile', 2, stage_off, BAR_STAGE, NP)
+    self.w('pending = true;')
+    self.close()
+    self.open('if (more)')
+    self.w(f'const size_t e0 = tile * {te}u;')
+    self.w('const size_t el = e0 + le;')
+    self.w('const bool active = lane_col && el < numElements && (flags == nullptr || flags[el] != 0u);')
+    # per term: the MMA thread starts on a term as soon as its slot is full
+    for ti, t in enumerate(s.terms):
+      self._lane(ti, t, slot_base[ti], lim, f'(ubuf{ti} + row * {pitch}u)', True)
+    self.close()
+    self.w('if (!more) break;')
+    self.w('prev_tile = tile; have_prev = true;')
+    self.close()
+    self.w('// a stage load still in flight after an abort must land before the CTA exits')
+    self.w(f'if (pending && !tfb_tc::mbar_wait(&bars[{BAR_STAGE}], it & 1u, {lim}ull)) atomicMax(&tfb_err_{b}, 41u);')
+    self.w('tfb_tc::cp_async_wait_all();')
+    self.w('if (ptid == 0) tfb_tc::bulk_wait();')
+    self.close()
+
   # ------------------------------------------------------------------ producer
   def _term(self, ti, t, slot_col, stage_off, lim, NP):
     b, LC = self.base, self.LC
@@ -577,14 +829,28 @@ class _TC:
       self.close()
       self.w(f'tfb_tc::named_sync(1, {NP});')
     # lane phase: wait for the slot, read the lane's column, split, store to TMEM
-    self.w(f'if (it > 0 && !tfb_tc::mbar_wait(&bars[{nterms + ti}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, {30 + ti}u); }}')
-    self.w('tfb_tc::fence_after();')
     if t.R is not None:
       src = f'({ubuf} + row * {pitch}u)'
       vec = True
     else:
       src = f'(cur + {stage_off[t.B.name]} + le * {bvals}u + lj * {t.K}u)'
       vec = t.K % 4 == 0
+    self._lane(ti, t, slot_col, lim, src, vec)
+    # the transposition buffer of this term is reused two terms later (or next term with one
+    # buffer), and the stage / buffers are reused after the last term
+    if self.sm['nbuf'] == 1 or ti == len(s.terms) - 1:
+      self.w(f'tfb_tc::named_sync(1, {NP});')
+    self.close()
+
+  def _lane(self, ti, t, slot_col, lim, src, vec):
+    """Lane phase of term ti: wait for its TMEM slot, read the lane's column of U_t from
+    `src`, split it into hi + lo and store both with tcgen05.st, then arrive on FULL[ti]."""
+    b, LC, H, prec = self.base, self.LC, self.H, self.prec
+    kp = self.lay['kpad'][ti]
+    acols = self.lay['a_cols'][ti]
+    nterms = len(self.s.terms)
+    self.w(f'if (it > 0 && !tfb_tc::mbar_wait(&bars[{nterms + ti}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, {30 + ti}u); }}')
+    self.w('tfb_tc::fence_after();')
     for ci, l0 in enumerate(range(0, kp, LC)):
       n = min(LC, kp - l0)
       real = max(0, min(n, t.K - l0))
@@ -630,13 +896,12 @@ class _TC:
     self.w('tfb_tc::st_wait();')
     self.w('tfb_tc::fence_before();')
     self.w(f'tfb_tc::mbar_arrive(&bars[{ti}]);')
-    # the transposition buffer of this term is reused two terms later (or next term with one
-    # buffer), and the stage / buffers are reused after the last term
-    if self.sm['nbuf'] == 1 or ti == len(s.terms) - 1:
-      self.w(f'tfb_tc::named_sync(1, {NP});')
-    self.close()
 
-  def _epilogue(self, d_main, d_corr, NP):
+  def _epilogue(self, d_main, d_corr, NP, sbuf='ubuf0', final_sync=True):
+    """Epilogue of the previous tile: accumulators -> registers (then FREE for the MMA), sum,
+    and either stage in `sbuf` + one bulk store (strided, aligned, unmasked output) or
+    per-lane stores. With final_sync=False the staging buffer's reuse is left to the caller.
+    """
     s = self.s
     M = s.M
     H = self.H
@@ -670,7 +935,7 @@ class _TC:
       for k in range(per):
         self.w(f'const unsigned q{k} = grp + {k * H}u;')
         self.open(f'if (q{k} < {nld}u)')
-        self.w(f'float* const dst = ubuf0 + row * {M}u + 8u * q{k};')
+        self.w(f'float* const dst = {sbuf} + row * {M}u + 8u * q{k};')
         if M % 8 == 0:
           self.w(f'reinterpret_cast<float4*>(dst)[0] = make_float4(__uint_as_float(dv[{8*k}]), __uint_as_float(dv[{8*k+1}]), __uint_as_float(dv[{8*k+2}]), __uint_as_float(dv[{8*k+3}]));')
           self.w(f'reinterpret_cast<float4*>(dst)[1] = make_float4(__uint_as_float(dv[{8*k+4}]), __uint_as_float(dv[{8*k+5}]), __uint_as_float(dv[{8*k+6}]), __uint_as_float(dv[{8*k+7}]));')
@@ -682,10 +947,11 @@ class _TC:
       self.w('tfb_tc::fence_proxy_async();')
       self.w(f'tfb_tc::named_sync(1, {NP});')
       self.open('if (ptid == 0)')
-      self.w(f'tfb_tc::bulk_store(obase, ubuf0, (unsigned)(nvalid * {out.element_volume() * 4}u));')
+      self.w(f'tfb_tc::bulk_store(obase, {sbuf}, (unsigned)(nvalid * {out.element_volume() * 4}u));')
       self.w('tfb_tc::bulk_wait_read();')
       self.close()
-      self.w(f'tfb_tc::named_sync(1, {NP});')
+      if final_sync:
+        self.w(f'tfb_tc::named_sync(1, {NP});')
       self.close()
       self.open('else if (pvalid && (flags == nullptr || flags[pel] != 0u))')
     else:

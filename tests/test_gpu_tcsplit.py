@@ -15,11 +15,11 @@ pytestmark = pytest.mark.gpu
 TOL = {'tf32x3': 1e-6, 'bf16x3': 5e-5}
 
 
-def _run(case, precision, n, seed=3, dist='uniform', use_flags=False):
+def _run(case, precision, n, seed=3, dist='uniform', use_flags=False, variant=None):
   import torch
   from tensorforge_b200.kernels import make
   from tensorforge_b200.runtime import compile_generator
-  g = make(case, 'float', precision=precision)
+  g = make(case, 'float', precision=precision, **({'variant': variant} if variant else {}))
   assert g.get_plan().strategy == 'tcsplit', g.get_plan()
   k = compile_generator(g)
   descrs = cases.build(case, cases.ns_from_module('tensorforge_b200'))
@@ -76,3 +76,34 @@ def test_other_shapes_split():
   got, ref, _, _ = _run('chain_o4_q27', 'tf32x3', 301)
   rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
   assert rel <= 1e-6, rel
+
+
+def _b_offset_seeds():
+  """Seeds whose random extra offset leaves the per-element B operand (Q, 504 values) 16-byte
+  aligned (staged with one bulk copy per tile) and misaligned (staged with cp.async)."""
+  descrs = cases.build('chain_o6', cases.ns_from_module('tensorforge_b200'))
+  found = {}
+  for seed in range(64):
+    lay = harness.make_layout(descrs, 8, seed)
+    b = [l for l in lay if l.kind == 'strided' and l.tensor.direction.name == 'SOURCE' and l.slot == 504]
+    found.setdefault(b[0].extra_offset % 4 == 0, seed)
+    if len(found) == 2:
+      return found[True], found[False]
+  raise AssertionError('no seed covers both staging paths')
+
+
+@pytest.mark.parametrize('aligned', [True, False])
+def test_chain_o6_bulk_and_fallback_staging(aligned):
+  seed = _b_offset_seeds()[0 if aligned else 1]
+  got, ref, _, _ = _run('chain_o6', 'tf32x3', 2999, seed=seed)
+  rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+  assert rel <= 1e-6, rel
+
+
+@pytest.mark.parametrize('precision', ['tf32x3', 'bf16x3'])
+def test_chain_o6_per_term_pipeline(precision):
+  """The per-term producer pipeline (plan option pipe=1), kept for shapes whose buffers
+  for the one-pass pipeline do not fit in shared memory."""
+  got, ref, _, _ = _run('chain_o6', precision, 1333, variant={'pipe': 1})
+  rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+  assert rel <= TOL[precision], rel
