@@ -281,7 +281,7 @@ def extra_workloads(stream, short=False):
                             'separate_launches_ms': ms2, 'separate_elements_per_s': total_el / (ms2 / 1e3)}
   # FP64 order-6 chain
   n = 100000 if short else 500000
-  for label, opts in (('fp64_plain', {}), ('fp64_dmma', {'precision': 'dmma'})):
+  for label, opts in (('fp64_colprog', {'variant': {'strategy': 'colprog'}}), ('fp64_dmma', {})):
     g = make(CASE, 'double', **opts)
     k = compile_generator(g)
     kw = {'numElements': n}

@@ -53,8 +53,9 @@ def emit_colprog(chain, plan, context, base_name, globals_):
   return _ColProg(chain, shape, plan, context, base_name).emit(globals_)
 
 
-def tile_elements(shape, threads):
-  return max(1, threads // shape.N)
+def tile_elements(shape, threads, cols=1):
+  """Elements per tile: `cols` columns per thread, whole elements of N columns each."""
+  return cols * max(1, threads // shape.N)
 
 
 class _ColProg:
@@ -74,8 +75,10 @@ class _ColProg:
     self.LC = plan.params['chunk']
     self.asrc = plan.params.get('a_source', 'const')
     self.prefetch = bool(plan.params.get('prefetch', 1)) and not getattr(self, 'grouped', False)
-    self.TE = tile_elements(shape, self.BT)
+    self.CPT = int(plan.params.get('cols', 1))
+    self.TE = tile_elements(shape, self.BT, self.CPT)
     self.TC = self.TE * shape.N
+    self.TCT = self.TC // self.CPT        # columns per round: thread t owns t + r * TCT
     self.kmax = max(t.K for t in shape.terms)
     self.pitch = _pad(self.kmax, self.VEC) + self.VEC
     self.lines = []
@@ -197,9 +200,11 @@ class _ColProg:
     s, T, BT = self.s, self.T, self.BT
     self.w(f'const unsigned le = threadIdx.x / {s.N}u, lj = threadIdx.x - le * {s.N}u;')
     self.w(f'const size_t e0 = tile * {self.TE}u;')
-    self.w('const size_t el = e0 + le;')
-    self.w(f'const bool lane_ok = threadIdx.x < {self.TC}u && el < numElements;')
-    self.w('const bool active = lane_ok && (flags == nullptr || flags[el] != 0u);')
+    for r in range(self.CPT):
+      sfx = '' if r == 0 else str(r)
+      self.w(f'const size_t el{sfx} = e0 + le + {r * (self.TCT // s.N)}u;')
+      self.w(f'const bool lane_ok{sfx} = threadIdx.x < {self.TCT}u && el{sfx} < numElements;')
+      self.w(f'const bool active{sfx} = lane_ok{sfx} && (flags == nullptr || flags[el{sfx}] != 0u);')
     for name, off in ([] if self.prefetch else self.r_off.items()):
       op = [o for o in self.chain.operands if o.name == name][0]
       nr = op.storage_size()
@@ -211,9 +216,11 @@ class _ColProg:
       self.close()
     if self.r_off and not self.prefetch:
       self.w('__syncthreads();')
-    self.w(f'{T} acc[{s.M}];')
-    self.w('#pragma unroll')
-    self.w(f'for (int i = 0; i < {s.M}; ++i) acc[i] = {self.lit(0)};')
+    for r in range(self.CPT):
+      a = 'acc' if r == 0 else f'acc{r}'
+      self.w(f'{T} {a}[{s.M}];')
+      self.w('#pragma unroll')
+      self.w(f'for (int i = 0; i < {s.M}; ++i) {a}[i] = {self.lit(0)};')
     for ti, t in enumerate(s.terms):
       self._term(ti, t)
     self._store()
@@ -409,28 +416,37 @@ class _ColProg:
       self._prefetch('tile + gridDim.x')
       self.close()
       self.w('tfb_cp::commit();')
-    # K stage
-    self.open('if (active)')
-    self.w(f'const {T}* const ucol = ubuf + threadIdx.x * {pitch}u;')
+    # K stage: each A value is an FMA operand for every column the thread owns
+    R = range(self.CPT)
+    sfx = lambda r: '' if r == 0 else str(r)
+    self.open('if (' + ' || '.join(f'active{sfx(r)}' for r in R) + ')')
+    for r in R:
+      self.w(f'const {T}* const ucol{sfx(r)} = ubuf + (threadIdx.x + {r * self.TCT}u) * {pitch}u;')
     cols = a_values(t)
     comps = ['x', 'y', 'z', 'w'][:VEC]
-    q = 0
-    cur = None
     for l0 in range(0, K, LC):
       n = min(LC, K - l0)
       self.open('')
-      self.w(f'{T} u[{n}];')
-      for v in range(n // VEC):
-        self.w(f'{{ const {VT} x = *reinterpret_cast<const {VT}*>(ucol + {l0 + v * VEC}); '
-               + ' '.join(f'u[{v * VEC + c}] = x.{comps[c]};' for c in range(VEC)) + ' }')
-      for i in range(n // VEC * VEC, n):
-        self.w(f'u[{i}] = ucol[{l0 + i}];')
+      for r in R:
+        u, uc = f'u{sfx(r)}', f'ucol{sfx(r)}'
+        self.w(f'{T} {u}[{n}];')
+        for v in range(n // VEC):
+          self.w(f'{{ const {VT} x = *reinterpret_cast<const {VT}*>({uc} + {l0 + v * VEC}); '
+                 + ' '.join(f'{u}[{v * VEC + c}] = x.{comps[c]};' for c in range(VEC)) + ' }')
+        for i in range(n // VEC * VEC, n):
+          self.w(f'{u}[{i}] = {uc}[{l0 + i}];')
       for l in range(l0, l0 + n):
         for (i, pos) in cols[l][1]:
-          if self.asrc == 'const':
-            self.w(f'acc[{i}] = {FMA}(cA_{b}[{self.a_base[ti] + pos}], u[{l - l0}], acc[{i}]);')
+          a = f'cA_{b}[{self.a_base[ti] + pos}]' if self.asrc == 'const' else f'sA[{self.a_base[ti] + pos}]'
+          if self.CPT == 1:
+            self.w(f'acc[{i}] = {FMA}({a}, u[{l - l0}], acc[{i}]);')
           else:
-            self.w(f'acc[{i}] = {FMA}(sA[{self.a_base[ti] + pos}], u[{l - l0}], acc[{i}]);')
+            self.open('')
+            self.w(f'const {T} av = {a};')
+            for r in R:
+              acc = f'acc{sfx(r)}'
+              self.w(f'{acc}[{i}] = {FMA}(av, u{sfx(r)}[{l - l0}], {acc}[{i}]);')
+            self.close()
       self.close()
     self.close()
     self.w('__syncthreads();')
@@ -441,18 +457,30 @@ class _ColProg:
     o = s.out
     M = s.M
     vol = o.element_volume()
+    sfx = lambda r: '' if r == 0 else str(r)
     coalesced = (o.addressing.name == 'STRIDED' and vol == M * s.N and vol % VEC == 0 and M % VEC == 0
                  and not s.accumulate)
+
+    def per_column():
+      for r in range(self.CPT):
+        self.open(f'if (active{sfx(r)})')
+        self.w(f'{T}* const col = {self._elem_ptr(o, "el" + sfx(r))} + (size_t)lj * {M}u;')
+        self.w('#pragma unroll')
+        op = '+=' if s.accumulate else '='
+        self.w(f'for (int i = 0; i < {M}; ++i) col[i] {op} acc{sfx(r)}[i];')
+        self.close()
+
     if coalesced:
       self.w('// stage the tile in shared memory, then write it back with coalesced 16-byte stores')
       self.w(f'{T}* const obase = {o.name} + e0 * {vol}u + {o.name}_extraOffset;')
       self.w(f'const bool vec_out = flags == nullptr && ((reinterpret_cast<uintptr_t>(obase) & 15u) == 0u);')
       self.open('if (vec_out)')
-      self.open('if (lane_ok)')
-      for v in range(M // VEC):
-        vals = ', '.join(f'acc[{v * VEC + c}]' for c in range(VEC))
-        self.w(f'reinterpret_cast<{VT}*>(ubuf + threadIdx.x * {M}u)[{v}] = make_{VT}({vals});')
-      self.close()
+      for r in range(self.CPT):
+        self.open(f'if (lane_ok{sfx(r)})')
+        for v in range(M // VEC):
+          vals = ', '.join(f'acc{sfx(r)}[{v * VEC + c}]' for c in range(VEC))
+          self.w(f'reinterpret_cast<{VT}*>(ubuf + (threadIdx.x + {r * self.TCT}u) * {M}u)[{v}] = make_{VT}({vals});')
+        self.close()
       self.w('__syncthreads();')
       self.w(f'const size_t nvalid = (numElements - e0) < {self.TE}u ? (numElements - e0) : {self.TE}u;')
       self.w(f'const unsigned nv = (unsigned)(nvalid * {vol // VEC}u);')
@@ -460,14 +488,8 @@ class _ColProg:
              f'reinterpret_cast<{VT}*>(obase)[q] = reinterpret_cast<const {VT}*>(ubuf)[q];')
       self.w('__syncthreads();')
       self.close()
-      self.open('else if (active)')
+      self.open('else')
+      per_column()
+      self.close()
     else:
-      self.open('if (active)')
-    self.w(f'{T}* const col = {self._elem_ptr(o, "el")} + (size_t)lj * {M}u;')
-    if s.accumulate:
-      self.w('#pragma unroll')
-      self.w(f'for (int i = 0; i < {M}; ++i) col[i] += acc[i];')
-    else:
-      self.w('#pragma unroll')
-      self.w(f'for (int i = 0; i < {M}; ++i) col[i] = acc[i];')
-    self.close()
+      per_column()

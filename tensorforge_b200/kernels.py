@@ -20,6 +20,7 @@ EXTRA = [
   ('chain_o6', 'float', {'precision': 'tf32x3', 'variant': {'pipe': 1}}),
   ('chain_o6', 'float', {'precision': 'bf16x3', 'variant': {'pipe': 1}}),
   ('chain_o6', 'double', {}),
+  ('chain_o6', 'double', {'variant': {'strategy': 'colprog'}}),
   ('chain_o6', 'double', {'precision': 'dmma'}),
   ('chain_o4_q27', 'double', {'precision': 'dmma'}),
   ('chain_o3_dense', 'double', {'precision': 'dmma'}),

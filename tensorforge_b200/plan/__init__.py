@@ -68,7 +68,9 @@ def make_plan(chain, context, variant=None):
           return p
         if forced == 'tcsplit':
           raise GenerationError('chain does not fit the tensor-core split form')
-      if precision == 'dmma' and context.fp_type == FloatingPointType.DOUBLE and forced != 'colprog':
+      # FP64: the DMMA tensor path is the default (exact FP64 products and sums, another
+      # summation order); the column program stays available as a forced variant
+      if precision in ('plain', 'dmma') and context.fp_type == FloatingPointType.DOUBLE and forced != 'colprog':
         p = chainplan.dmma_plan(chain, shape, variant)
         if p is not None:
           return p

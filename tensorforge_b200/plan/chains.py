@@ -149,20 +149,27 @@ def r_slots(term):
 # this many the instruction stream outgrows the SM's instruction caches and ptxas time grows
 # to minutes per kernel, so such chains go to the generic generator.
 COLPROG_MAX_FMAS = 6144
+# A values as constant-bank FMA operands stay in the immediate-constant cache up to roughly
+# this many values. Measured on B200: constant A is fastest for most random chains with at
+# most 2,048 values and for the dense 56x56 GEMM (3,136 values: 2.54e8 vs 2.32e8 el/s);
+# the order-6 chain (4,253 values over three terms) runs 1.24x faster from shared memory.
+COLPROG_CONST_A = 4096
 
 
 def colprog_plan(chain, shape: LeftChain, fp_size, variant):
   from ..codegen.colprog import tile_elements
   threads = variant.get('threads', 128)
   chunk = variant.get('chunk', 16)
-  a_source = variant.get('a_source', 'const')
+  a_total = sum(t.A.storage_size() for t in shape.terms)
+  a_source = variant.get('a_source', 'const' if a_total <= COLPROG_CONST_A else 'smem')
   vec = 4 if fp_size == 4 else 2
   chunk = max(vec, (chunk + vec - 1) // vec * vec)
   if shape.M > 128 or shape.N > threads:
     return None
   if sum(t.A.storage_size() for t in shape.terms) > COLPROG_MAX_FMAS:
     return None
-  te = tile_elements(shape, threads)
+  cols = int(variant.get('cols', 1))
+  te = tile_elements(shape, threads, cols)
   kmax = max(t.K for t in shape.terms)
   pitch = (kmax + vec - 1) // vec * vec + vec
   a_vals = sum(t.A.storage_size() for t in shape.terms)
@@ -182,8 +189,11 @@ def colprog_plan(chain, shape: LeftChain, fp_size, variant):
                            if o is not None and o.kind == 'batched'}.values()) * fp_size
     if smem > SMEM_LIMIT:
       prefetch = 0
-  return Plan('colprog', {'threads': threads, 'chunk': chunk, 'min_blocks': variant.get('min_blocks', 0),
-                          'a_source': a_source, 'prefetch': prefetch},
+  params = {'threads': threads, 'chunk': chunk, 'min_blocks': variant.get('min_blocks', 0),
+            'a_source': a_source, 'prefetch': prefetch}
+  if cols != 1:
+    params['cols'] = cols
+  return Plan('colprog', params,
               smem, threads, note=f'M={shape.M} N={shape.N} terms={len(shape.terms)} tile={te}')
 
 
