@@ -362,11 +362,13 @@ def impl_ours(args, rank, world, dist):
   h2d = sum(host[x].numel() * host[x].element_size() for x in inputs)
   d2h = host[outname].numel() * host[outname].element_size()
 
+  # slices of the batch flow through three streams: copy-in, kernel and copy-out overlap
+  from tensorforge_b200.runtime.pipeline import HostPipeline
+  pipe = HostPipeline(k, gen, slices=8, streams=3)
+  dev_bufs = {t.name: kw[t.name] for t, _ in gen.abi_symbols()}
+
   def e2e_step():
-    for x in inputs:
-      kw[x].copy_(host[x], non_blocking=True)
-    k(**kw)
-    host[outname].copy_(kw[outname], non_blocking=True)
+    pipe(host, dev_bufs, n)
 
   e_steps = max(2, min(args.steps, 5))
   e_total, _ = time_launches(e2e_step, stream, e_steps, 1, dist)
@@ -427,7 +429,7 @@ def impl_ours(args, rank, world, dist):
     'roofline': roofline,
     'cpu_baseline': cpu,
     'e2e': {'value': world * n / (e_ms / 1e3), 'unit': 'elements/s', 'h2d_bytes_per_step': h2d,
-            'd2h_bytes_per_step': d2h},
+            'd2h_bytes_per_step': d2h, 'api': 'runtime.pipeline.HostPipeline (8 slices, 3 streams)'},
     'gpu_launches': args.steps,
     'clocks': clocks.summary(),
   }

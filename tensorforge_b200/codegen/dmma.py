@@ -17,6 +17,10 @@ multiple of 8):
      with coalesced stores (accumulated into out_e when the chain adds, skipped for
      elements whose flag is 0).
 
+With plan option prefetch=1 (the default when it fits in shared memory) the next tile's
+batched B and R values are copied into a stage with cp.async right after the U phase has
+consumed it, so the loads overlap the MMA phase and the epilogue.
+
 Pitches: LD = 4 (mod 8) doubles makes both fragment loads (lane -> row lane/4, k lane%4)
 bank-conflict free; LDO = 2 (mod 4) does the same for the epilogue's fragment stores.
 Padded k rows of U and A stay zero, so K need not be a multiple of 4. The contraction
@@ -46,8 +50,24 @@ def _pad(x, m):
   return (x + m - 1) // m * m
 
 
-def layout(shape, te):
-  """Pitches and shared-memory regions (in doubles) for a tile of `te` elements."""
+def staged_ops(shape):
+  """Distinct batched operands a tile reads: [(operand, values per element)], B before R."""
+  out = []
+  for role in ('B', 'R'):
+    for t in shape.terms:
+      op = getattr(t, role)
+      if op is None or op.kind != 'batched' or any(op is o for o, _ in out):
+        continue
+      out.append((op, op.storage_size() if op.sparse else op.element_volume()))
+  return out
+
+
+def layout(shape, te, prefetch=False):
+  """Pitches and shared-memory regions (in doubles) for a tile of `te` elements.
+
+  With prefetch, the next tile's batched B and R values are copied with cp.async into a
+  stage region while the current tile's MMAs run; R is then read from the stage.
+  """
   M, N = shape.M, shape.N
   kp = _pad(max(t.K for t in shape.terms), 4)
   ld = kp if kp % 8 == 4 else kp + 4
@@ -65,8 +85,15 @@ def layout(shape, te):
       r_off[t.R.name] = r_vals
       r_vals += te * _pad(t.R.storage_size(), 2)
   region = max(u_vals, o_vals)
+  stage_off, stage = {}, 0
+  if prefetch:
+    r_vals, r_off = 0, {}
+    for op, vals in staged_ops(shape):
+      stage_off[op.name] = stage
+      stage += te * _pad(vals, 2)
   return dict(KP=kp, LD=ld, MP=mp, LDO=ldo, C=C, A=a_vals, U=u_vals, O=o_vals, R=r_vals, r_off=r_off,
-              region=region, total=a_vals + region + r_vals)
+              region=region, stage=stage, stage_off=stage_off, prefetch=prefetch,
+              total=a_vals + region + r_vals + stage)
 
 
 def plan(chain, shape, variant, smem_limit):
@@ -77,12 +104,17 @@ def plan(chain, shape, variant, smem_limit):
     return None
   te0 = 8 // gcd(N, 8)
   target = variant.get('columns', 72)
-  te = variant.get('tile_elements') or max(te0, (target // N) // te0 * te0)
-  while te >= te0:
-    lay = layout(shape, te)
-    if lay['total'] * 8 <= smem_limit:
+  te_max = variant.get('tile_elements') or max(te0, (target // N) // te0 * te0)
+  lay = None
+  for prefetch in ((1, 0) if variant.get('prefetch', 1) else (0,)):
+    te = te_max
+    while te >= te0:
+      lay = layout(shape, te, bool(prefetch))
+      if lay['total'] * 8 <= smem_limit:
+        break
+      te -= te0
+    if te >= te0:
       break
-    te -= te0
   else:
     return None
   mb = lay['MP'] // 8
@@ -92,7 +124,7 @@ def plan(chain, shape, variant, smem_limit):
   threads = 32 * mb * ns
   if threads > 1024:
     return None
-  return Plan('dmma', {'tile_elements': te, 'nsplit': ns}, lay['total'] * 8, threads,
+  return Plan('dmma', {'tile_elements': te, 'nsplit': ns, 'prefetch': prefetch}, lay['total'] * 8, threads,
               note=f'M={M} N={N} terms={len(shape.terms)} C={lay["C"]} warps={mb * ns}')
 
 
@@ -107,7 +139,7 @@ class _Dmma:
     self.chain, self.s, self.plan, self.ctx, self.base = chain, shape, plan_, ctx, base
     self.TE = plan_.params['tile_elements']
     self.NS = plan_.params['nsplit']
-    self.L = layout(shape, self.TE)
+    self.L = layout(shape, self.TE, bool(plan_.params.get('prefetch', 0)))
     self.MB = self.L['MP'] // 8
     self.NB = self.L['C'] // 8
     self.BT = 32 * self.MB * self.NS
@@ -187,6 +219,34 @@ class _Dmma:
       self.w(f'sR[{off} + ei * {nrp}u + p] = live ? __ldg({self._elem_ptr(op, "e")} + p) : 0.0;')
       self.close()
 
+  def _prefetch(self, tile_expr):
+    """cp.async the tile's batched B / R values into the stage (16-byte chunks when aligned)."""
+    L, BT, TE = self.L, self.BT, self.TE
+    for op, vals in staged_ops(self.s):
+      off = L['stage_off'][op.name]
+      vp = _pad(vals, 2)
+      self.open('')
+      self.w(f'const size_t pe0 = ({tile_expr}) * {TE}u;')
+      pairs = vals // 2
+      if pairs:
+        self.open(f'for (unsigned q = threadIdx.x; q < {TE * pairs}u; q += {BT}u)')
+        self.w(f'const unsigned ei = q / {pairs}u, c2 = q - ei * {pairs}u;')
+        self.w('const size_t ee = pe0 + ei;')
+        self.open('if (ee < numElements && (flags == nullptr || flags[ee] != 0u))')
+        self.w(f'const double* src = {self._elem_ptr(op, "ee")} + 2u * c2;')
+        self.w(f'double* dst = sS + {off}u + ei * {vp}u + 2u * c2;')
+        self.w('if ((reinterpret_cast<uintptr_t>(src) & 15u) == 0u) tfb_cp::copy16(dst, src);')
+        self.w('else { tfb_cp::copy8(dst, src); tfb_cp::copy8(dst + 1, src + 1); }')
+        self.close()
+        self.close()
+      if vals % 2:
+        self.open(f'for (unsigned ei = threadIdx.x; ei < {TE}u; ei += {BT}u)')
+        self.w('const size_t ee = pe0 + ei;')
+        self.w(f'if (ee < numElements && (flags == nullptr || flags[ee] != 0u)) '
+               f'tfb_cp::copy8(sS + {off}u + ei * {vp}u + {vals - 1}u, {self._elem_ptr(op, "ee")} + {vals - 1}u);')
+        self.close()
+      self.close()
+
   def _u_phase(self):
     """U_t[c][l] = sum_m B_t[l][m] * R_t[m][j] for c = e*N + j; terms sharing B load it once."""
     s, L, BT, TE = self.s, self.L, self.BT, self.TE
@@ -203,9 +263,15 @@ class _Dmma:
       self.w(f'const unsigned ei = q / {KP}u, l = q - ei * {KP}u;')
       self.w('const size_t e = e0 + ei;')
       self.w(f'const bool live = l < {K}u && e < numElements && (flags == nullptr || flags[e] != 0u);')
-      self.w(f'const double* const bq = live ? {self._elem_ptr(B, "e")} + l : nullptr;')
-      for m in range(P):
-        self.w(f'const double q{m} = live ? __ldg(bq + {m * K}u) : 0.0;')
+      if L['prefetch']:
+        bvp = _pad(B.element_volume(), 2)
+        self.w(f'const double* const bq = sS + {L["stage_off"][B.name]}u + ei * {bvp}u + (live ? l : 0u);')
+        for m in range(P):
+          self.w(f'const double q{m} = live ? bq[{m * K}u] : 0.0;')
+      else:
+        self.w(f'const double* const bq = live ? {self._elem_ptr(B, "e")} + l : nullptr;')
+        for m in range(P):
+          self.w(f'const double q{m} = live ? __ldg(bq + {m * K}u) : 0.0;')
       for ti, t in terms:
         self.w(f'double* const urow{ti} = sU + {ti * C * LD}u + ei * {N * LD}u + l;')
         if t.R is None:
@@ -214,7 +280,10 @@ class _Dmma:
           continue
         if t.R.kind == 'batched':
           nrp = _pad(t.R.storage_size(), 2)
-          self.w(f'const double* const rq{ti} = sR + {L["r_off"][t.R.name]}u + ei * {nrp}u;')
+          if L['prefetch']:
+            self.w(f'const double* const rq{ti} = sS + {L["stage_off"][t.R.name]}u + ei * {nrp}u;')
+          else:
+            self.w(f'const double* const rq{ti} = sR + {L["r_off"][t.R.name]}u + ei * {nrp}u;')
           rv = lambda pos, ti=ti: f'rq{ti}[{pos}]'
         else:
           rv = lambda pos, t=t: f'__ldg({t.R.name} + {pos})'
@@ -285,6 +354,9 @@ class _Dmma:
     s, L, BT, TE, b = self.s, self.L, self.BT, self.TE, self.base
     kname = f'kernel_{b}'
     self.w(DMMA_HELPERS)
+    if self.L['prefetch']:
+      from .colprog import CP_HELPERS
+      self.w(CP_HELPERS)
     self.w(f'// generated by tensorforge_b200 (strategy: dmma, tile={TE} elements, C={L["C"]} columns, '
            f'{self.MB}x{self.NS} warps, LD={L["LD"]}, LDO={L["LDO"]})')
     self.w('// meta data:')
@@ -300,21 +372,40 @@ class _Dmma:
     self.w('double* const sA = smem;')
     self.w(f'double* const sU = smem + {L["A"]};')
     self.w(f'double* const sR = smem + {L["A"] + L["region"]};')
+    if L['prefetch']:
+      self.w(f'double* const sS = smem + {L["A"] + L["region"] + L["R"]};')
     self.w(f'const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;')
     self.w(f'const unsigned mb = warp % {self.MB}u, ns = warp / {self.MB}u;')
     self.w('const unsigned fr = lane >> 2, fq = lane & 3u;')
     self._stage_a()
     self.w(f'const size_t numTiles = (numElements + {TE - 1}u) / {TE}u;')
+    pf = L['prefetch']
+    if pf:
+      self.open('if (blockIdx.x < numTiles)')
+      self._prefetch('(size_t)blockIdx.x')
+      self.close()
+      self.w('tfb_cp::commit();')
     self.open('for (size_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x)')
     self.w(f'const size_t e0 = tile * {TE}u;')
-    if L['r_off']:
+    if pf:
+      self.w('tfb_cp::wait_all();')
+      self.w('__syncthreads();')
+    elif L['r_off']:
       self._stage_r()
       self.w('__syncthreads();')
     self._u_phase()
     self.w('__syncthreads();')
+    if pf:
+      self.w('// the stage is consumed: fetch the next tile while the MMAs run')
+      self.open('if (tile + gridDim.x < numTiles)')
+      self._prefetch('tile + gridDim.x')
+      self.close()
+      self.w('tfb_cp::commit();')
     self._mma_phase()
     self._epilogue()
     self.close()
+    if pf:
+      self.w('tfb_cp::wait_all();')
     self.ind -= 1
     self.w('}')
     return '\n'.join(self.lines), self._launch(globals_, kname), ''

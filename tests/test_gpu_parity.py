@@ -90,3 +90,28 @@ def test_alpha_is_applied():
     if l.kind == 'strided' and l.tensor.direction.name != 'SOURCE':
       got = dev[l.name].double().cpu().numpy()
       assert np.abs(got - mem.buffers[l.name]).max() <= 1e-5 * np.abs(mem.buffers[l.name]).max()
+
+
+COLPROG_VARIANTS = [
+  {'strategy': 'colprog', 'a_source': 'const'},
+  {'strategy': 'colprog', 'a_source': 'smem'},
+  {'strategy': 'colprog', 'a_source': 'smem', 'cols': 2},
+  {'strategy': 'colprog', 'a_source': 'const', 'prefetch': 0, 'threads': 256},
+]
+
+
+@pytest.mark.parametrize('variant', COLPROG_VARIANTS, ids=lambda v: ','.join(f'{k}={x}' for k, x in v.items() if k != 'strategy'))
+@pytest.mark.parametrize('case', ['chain_o6', 'c0_gemm_ptr'])
+def test_column_program_variants_match_reference(case, variant):
+  """Every column-program variant the planner or the tuner can pick, on the golden vectors."""
+  from tensorforge_b200.common.context import Options
+  paths = [p for p in golden_files() if load(p)[1]['case'] == case and load(p)[1]['fp'] == 'float']
+  assert paths
+  z, meta = load(paths[0])
+  out = _run_case(meta, z, Options(variant=variant))
+  for s in meta['symbols']:
+    if s['kind'] in ('scalar', 'shared'):
+      continue
+    ref = z[f'out_{s["name"]}'].astype(np.float64)
+    scale = max(1e-30, float(np.abs(ref).max()))
+    assert np.abs(out[s['name']] - ref).max() <= 1e-5 * scale, s['name']
