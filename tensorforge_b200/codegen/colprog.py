@@ -424,9 +424,23 @@ class _ColProg:
       self.w(f'const {T}* const ucol{sfx(r)} = ubuf + (threadIdx.x + {r * self.TCT}u) * {pitch}u;')
     cols = a_values(t)
     comps = ['x', 'y', 'z', 'w'][:VEC]
+    # shared-memory A is consumed in storage order: fetch it one aligned vector at a time
+    # (one broadcast LDS.128 / LDS.64 per VEC values) instead of one load per value
+    loaded = set()
+
+    def a_operand(pos):
+      if self.asrc == 'const':
+        return f'cA_{b}[{self.a_base[ti] + pos}]'
+      g = self.a_base[ti] + pos
+      v = g // VEC
+      if v not in loaded:
+        loaded.add(v)
+        self.w(f'const {VT} av{v} = reinterpret_cast<const {VT}*>(sA)[{v}];')
+      return f'av{v}.{comps[g % VEC]}'
     for l0 in range(0, K, LC):
       n = min(LC, K - l0)
       self.open('')
+      loaded.clear()  # vectors are declared per chunk block
       for r in R:
         u, uc = f'u{sfx(r)}', f'ucol{sfx(r)}'
         self.w(f'{T} {u}[{n}];')
@@ -437,7 +451,7 @@ class _ColProg:
           self.w(f'{u}[{i}] = {uc}[{l0 + i}];')
       for l in range(l0, l0 + n):
         for (i, pos) in cols[l][1]:
-          a = f'cA_{b}[{self.a_base[ti] + pos}]' if self.asrc == 'const' else f'sA[{self.a_base[ti] + pos}]'
+          a = a_operand(pos)
           if self.CPT == 1:
             self.w(f'acc[{i}] = {FMA}({a}, u[{l - l0}], acc[{i}]);')
           else:
