@@ -851,6 +851,36 @@ class _TC:
     nterms = len(self.s.terms)
     self.w(f'if (it > 0 && !tfb_tc::mbar_wait(&bars[{nterms + ti}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, {30 + ti}u); }}')
     self.w('tfb_tc::fence_after();')
+    if self.pipe == 2 and prec == 'tf32x3' and vec and t.K % 4 == 0 and LC == 16 and -(-kp // LC) <= H:
+      # one body for all groups: group g takes columns [16 g, 16 g + 16) of the slot (keeps
+      # the instruction footprint of the lane phase to one copy per term)
+      self.open('')
+      self.w('const unsigned c0 = grp * 16u;')
+      self.open(f'if (c0 < {kp}u)')
+      self.w('float u[16];')
+      self.w('#pragma unroll')
+      self.w('for (int i = 0; i < 16; ++i) u[i] = 0.0f;')
+      self.open('if (active)')
+      self.w(f'const float* p = {src} + c0;')
+      for v in range(4):
+        self.w(f'if (c0 + {4 * v}u < {t.K}u) {{ const float4 x = *reinterpret_cast<const float4*>(p + {4 * v}); '
+               f'u[{4*v}] = x.x; u[{4*v+1}] = x.y; u[{4*v+2}] = x.z; u[{4*v+3}] = x.w; }}')
+      self.close()
+      self.w('unsigned hv[16], lv[16];')
+      self.w('#pragma unroll')
+      self.w('for (int i = 0; i < 16; ++i) { hv[i] = tfb_tc::tf32_rna(u[i]); lv[i] = __float_as_uint(u[i] - __uint_as_float(hv[i])); }')
+      self.w(f'tfb_tc::st_x8(lane_addr + {slot_col}u + c0, hv);')
+      self.w(f'tfb_tc::st_x8(lane_addr + {slot_col + acols}u + c0, lv);')
+      self.open(f'if (c0 + 8u < {kp}u)')
+      self.w(f'tfb_tc::st_x8(lane_addr + {slot_col + 8}u + c0, hv + 8);')
+      self.w(f'tfb_tc::st_x8(lane_addr + {slot_col + acols + 8}u + c0, lv + 8);')
+      self.close()
+      self.close()
+      self.close()
+      self.w('tfb_tc::st_wait();')
+      self.w('tfb_tc::fence_before();')
+      self.w(f'tfb_tc::mbar_arrive(&bars[{ti}]);')
+      return
     for ci, l0 in enumerate(range(0, kp, LC)):
       n = min(LC, kp - l0)
       real = max(0, min(n, t.K - l0))
