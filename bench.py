@@ -98,19 +98,28 @@ class Clocks:
 
 # ----------------------------------------------------------------------------- data
 
-def make_inputs(gen, n, device, seed):
-  """Device buffers in the launcher's ABI layout for the order-6 chain."""
+def make_inputs(gen, n, device, seed, dist='uniform', dtype=None):
+  """Device buffers in the launcher's ABI layout for the order-6 chain.
+
+  dist 'uniform': U(-1, 1); 'loguniform': random sign times 10^U(-3, 3) (magnitudes over
+  six decades, the precision workload)."""
   import torch
   g = torch.Generator(device=device)
   g.manual_seed(seed)
+  dtype = dtype or torch.float32
+
+  def values(size):
+    if dist == 'loguniform':
+      mag = torch.pow(10.0, torch.rand(size, generator=g, device=device, dtype=torch.float64) * 6 - 3)
+      sign = torch.where(torch.rand(size, generator=g, device=device) < 0.5, -1.0, 1.0).double()
+      return (mag * sign).to(dtype)
+    return (torch.rand(size, generator=g, device=device, dtype=dtype) * 2 - 1)
   bufs = {}
   for t, stype in gen.abi_symbols():
     if t.addressing.name == 'NONE':
-      size = t.spp.count_nz()
-      bufs[t.name] = torch.rand(size, generator=g, device=device) * 2 - 1
+      bufs[t.name] = values(t.spp.count_nz())
     else:
-      vol = t.get_real_volume()
-      bufs[t.name] = torch.rand(n * vol, generator=g, device=device) * 2 - 1
+      bufs[t.name] = values(n * t.get_real_volume())
   return bufs
 
 
@@ -276,9 +285,40 @@ def extra_workloads(stream, short=False):
       k(**kw)
   total2, per2 = time_launches(separate, stream, 5, 2)
   ms2 = sum(per2) / len(per2)
+  per_group = []
+  for i, (b, q, n) in enumerate(groups):  # the same launch with every other group emptied
+    one = gk.prepare([dict(kw, numElements=(kw['numElements'] if j == i else 0)) for j, kw in enumerate(kws)])
+    _, pg = time_launches(one.launch, stream, 3, 1)
+    g_ms = sum(pg) / len(pg)
+    g_nz = n * gk.gens[i].get_chain().nz_flops_per_element()
+    per_group.append({'basis': b, 'quantities': q, 'elements': n, 'ms': g_ms, 'elements_per_s': n / (g_ms / 1e3),
+                      'nz_gflops': g_nz / (g_ms / 1e3) / 1e9})
   out['c3_mixed_shapes'] = {'elements': total_el, 'groups': len(groups), 'elements_per_s': total_el / (ms / 1e3),
                             'nz_gflops': nz / (ms / 1e3) / 1e9, 'ms': ms, 'launch': 'one persistent kernel, CUDA graph replay',
-                            'separate_launches_ms': ms2, 'separate_elements_per_s': total_el / (ms2 / 1e3)}
+                            'separate_launches_ms': ms2, 'separate_elements_per_s': total_el / (ms2 / 1e3),
+                            'per_group': per_group}
+  # config 2: log-uniform magnitudes through every precision variant, error vs the FP64 oracle
+  descrs = cases.build(CASE, cases.ns_from_module('tensorforge_b200'))
+  n2 = 100000 if short else 500000
+  c2 = {}
+  for label, fp, opts in (('fp32_plain', 'float', {}), ('tf32x3', 'float', {'precision': 'tf32x3'}),
+                          ('bf16x3', 'float', {'precision': 'bf16x3'}),
+                          ('fp64_colprog', 'double', {'variant': {'strategy': 'colprog'}}),
+                          ('fp64_dmma', 'double', {})):
+    g = make(CASE, fp, **opts)
+    k = compile_generator(g)
+    kw = make_inputs(g, n2, dev, 7, 'loguniform', torch.float64 if fp == 'double' else torch.float32)
+    kw['numElements'] = n2
+    k(**kw)
+    torch.cuda.synchronize()
+    acc = check_accuracy(descrs, g, kw, 2048)
+    total, per = time_launches(lambda: k(**kw), stream, 5, 2)
+    ms = sum(per) / len(per)
+    c2[label] = {'elements_per_s': n2 / (ms / 1e3), 'plan': g.get_plan().key(), 'rel_l2': acc['rel_l2'],
+                 'max_abs': acc['max_abs'], 'ref_max_abs': acc['ref_max_abs']}
+    del kw
+  out['c2_precision_loguniform'] = {'elements': n2, 'values': 'sign * 10^U(-3,3), seed 7', 'variants': c2}
+  torch.cuda.empty_cache()
   # FP64 order-6 chain
   n = 100000 if short else 500000
   for label, opts in (('fp64_colprog', {'variant': {'strategy': 'colprog'}}), ('fp64_dmma', {})):
