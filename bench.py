@@ -338,6 +338,7 @@ def extra_workloads(stream, short=False):
 
 def impl_ours(args, rank, world, dist):
   import torch
+  from tensorforge_b200.runtime import ranks
   from tensorforge_b200 import workloads as cases
   from tensorforge_b200.kernels import make
   from tensorforge_b200.runtime import compile_generator
@@ -352,7 +353,7 @@ def impl_ours(args, rank, world, dist):
   stream = torch.cuda.current_stream()
   primary = None
   ref_gen = make(CASE, 'float')
-  bufs = make_inputs(ref_gen, n, device, seed=1234 + rank)
+  bufs = make_inputs(ref_gen, n, device, seed=ranks.rank_seed(1234, rank))
   outname = [t.name for t, _ in ref_gen.abi_symbols() if t.direction != DataFlowDirection.SOURCE][0]
   descrs = cases.build(CASE, cases.ns_from_module('tensorforge_b200'))
   extra = ['plain'] if 'plain' not in variants else []
@@ -378,6 +379,9 @@ def impl_ours(args, rank, world, dist):
     results[name] = {'kernel': gen.get_base_name(), 'plan': gen.get_plan().key(), 'ms_total': total,
                      'launch_ms': per, 'accuracy': acc, 'gen': gen, 'k': k, 'kw': kw}
     ok = name == 'plain' or acc['rel_l2'] <= 1e-6
+    if primary is None:
+      # the choice changes the collective sequence (timed barriers): every rank must agree
+      ok = ranks.all_ranks(ok, dist)
     if primary is None and ok:
       primary = name
     log(f'{name}: {n / (total / steps / 1e3):.3e} el/s, rel_l2 {acc["rel_l2"]:.2e}, plan {gen.get_plan().key()}')
@@ -389,12 +393,8 @@ def impl_ours(args, rank, world, dist):
   # the timed region of record: K steps of the primary variant, clocks sampled meanwhile
   with Clocks(index=torch.cuda.current_device()) as clocks:
     total, per = time_launches(lambda: k(**kw), stream, args.steps, args.warmup, dist)
-  ms = total / args.steps
-  if dist is not None:
-    t = torch.tensor([ms], device=device, dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
-  value = world * n / (ms / 1e3)
+  ms = ranks.max_over_ranks(total / args.steps, dist)
+  value = ranks.aggregate_rate(world, n, ms)
 
   # end to end through the C-ABI launcher with host buffers (pinned), copies inside the timed region
   host = {name: b.cpu().pin_memory() for name, b in bufs.items()}
@@ -412,11 +412,7 @@ def impl_ours(args, rank, world, dist):
 
   e_steps = max(2, min(args.steps, 5))
   e_total, _ = time_launches(e2e_step, stream, e_steps, 1, dist)
-  e_ms = e_total / e_steps
-  if dist is not None:
-    t = torch.tensor([e_ms], device=device, dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e_ms = float(t.item())
+  e_ms = ranks.max_over_ranks(e_total / e_steps, dist)
 
   if rank != 0:
     return
@@ -491,20 +487,14 @@ def main():
   ap.add_argument('--no-cpu', action='store_true')
   ap.add_argument('--no-extras', action='store_true')
   args = ap.parse_args()
-  rank = int(os.environ.get('RANK', '0'))
-  world = int(os.environ.get('WORLD_SIZE', '1'))
+  from tensorforge_b200.runtime import ranks
+  rank, world, _ = ranks.env_rank()
   if args.impl == 'reference':
     impl_reference(args, rank, world)
     return
   import torch
-  dist = None
-  if world > 1:
-    import datetime
-    import torch.distributed as tdist
-    torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', '0')))
-    tdist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
-    dist = tdist
-  else:
+  dist = ranks.init('nccl')
+  if dist is None:
     torch.cuda.set_device(0)
   try:
     impl_ours(args, rank, world, dist)
