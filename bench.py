@@ -233,6 +233,17 @@ def impl_reference(args, rank, world):
 
 # ----------------------------------------------------------------------------- ours
 
+_FP32_PEAK = []
+
+
+def fp32_peak_cached():
+  """FP32 FFMA peak measured once per run (the probe of the native runtime library)."""
+  if not _FP32_PEAK:
+    from tensorforge_b200.runtime.peaks import fma_peak
+    _FP32_PEAK.append(fma_peak('float'))
+  return _FP32_PEAK[0]
+
+
 def extra_workloads(stream, short=False):
   """Secondary BASELINE configs measured next to the headline (device-resident inputs)."""
   import torch
@@ -259,8 +270,15 @@ def extra_workloads(stream, short=False):
     total, per = time_launches(lambda: k(**kw), stream, 10, 3)
     ms = sum(per) / len(per)
     flops = n * g.get_chain().nz_flops_per_element()
+    # both bounds: FP32 pipe (56,448 flops per element) and HBM (4,048 bytes: B, C, 2 pointers)
+    bytes_el = g.get_chain().bytes_per_element()
+    fp32 = fp32_peak_cached()
+    hbm = peaks()[0]['hbm_gbs'] * 1e9
     out[f'c0_gemm_{n}'] = {'elements_per_s': n / (ms / 1e3), 'gflops': flops / (ms / 1e3) / 1e9, 'ms': ms,
-                           'plan': g.get_plan().key()}
+                           'plan': g.get_plan().key(),
+                           'roofline': {'fp32_bound_el_s': fp32 / (flops / n), 'hbm_bound_el_s': hbm / bytes_el,
+                                        'frac_of_tighter': (n / (ms / 1e3)) / min(fp32 / (flops / n), hbm / bytes_el),
+                                        'bytes_per_element': bytes_el, 'flops_per_element': flops / n}}
   # config 3: mixed shapes, one persistent launch over a work table, replayed from a CUDA graph
   from tensorforge_b200.kernels import grouped_catalogue
   gk = dict(grouped_catalogue())['bench_c3']
@@ -439,14 +457,14 @@ def impl_ours(args, rank, world, dist):
   extra_out = {}
   if plain is not None:
     p_launch = sum(plain['launch_ms']) / len(plain['launch_ms'])
-    from tensorforge_b200.runtime.peaks import fma_peak
-    fp32_peak = fma_peak('float')
+    fp32_peak = fp32_peak_cached()
     p_flops = n * nz / (p_launch / 1e3)
     extra_out['plain_fp32'] = {
       'elements_per_s': n / (p_launch / 1e3), 'kernel': plain['kernel'], 'plan': plain['plan'],
       'accuracy': plain['accuracy'],
       'roofline': {'bound': 'fp32', 'achieved': p_flops / 1e12, 'peak': fp32_peak / 1e12, 'unit': 'TFLOP/s',
                    'frac': p_flops / fp32_peak, 'flops_per_element': nz,
+                   'dense_equivalent_flops_per_element': chain.dense_flops_per_element(),
                    'peak_source': 'measured FP32 FFMA probe (libtfb200_runtime tfb_fma_peak_launch), same run'}}
   for name, r in results.items():
     extra_out.setdefault('variants', {})[name] = {

@@ -18,6 +18,11 @@ EXTRA = [
   ('chain_o6', 'float', {'precision': 'bf16x3'}),
   ('chain_o4_q27', 'float', {'precision': 'tf32x3'}),
   ('chain_o6', 'float', {'precision': 'tf32x3', 'variant': {'pipe': 1}}),
+  ('c0_gemm_ptr', 'float', {'precision': 'tf32x3'}),
+  ('c0_gemm_strided', 'float', {'precision': 'tf32x3'}),
+  ('gemm_add', 'float', {'precision': 'tf32x3'}),
+  ('chain_o3_dense', 'float', {'precision': 'tf32x3'}),
+  ('sparse_a_shared', 'float', {'precision': 'tf32x3'}),
   ('chain_o6', 'float', {'precision': 'bf16x3', 'variant': {'pipe': 1}}),
   ('chain_o6', 'double', {}),
   ('chain_o6', 'double', {'variant': {'strategy': 'colprog'}}),

@@ -25,11 +25,20 @@ def _run(case, precision, n, seed=3, dist='uniform', use_flags=False, variant=No
   descrs = cases.build(case, cases.ns_from_module('tensorforge_b200'))
   lay, mem = harness.make_memory(descrs, n, seed=seed, dist=dist)
   flags = harness.make_flags(n, seed) if use_flags else None
-  dev, kw = {}, {'numElements': n}
+  dev, kw, keep = {}, {'numElements': n}, []
   for l in lay:
+    if l.kind == 'scalar':
+      kw[l.name] = float(mem.scalars[l.name])
+      continue
     dev[l.name] = torch.tensor(mem.buffers[l.name], dtype=torch.float32, device='cuda')
     kw[l.name] = dev[l.name]
     if l.kind == 'strided':
+      kw[f'{l.name}_extraOffset'] = l.extra_offset
+    elif l.kind == 'ptr':  # device array of element pointers (without the extra offset)
+      starts = np.asarray(l.starts, dtype=np.int64) - l.extra_offset
+      ptrs = torch.tensor(dev[l.name].data_ptr() + starts * 4, dtype=torch.int64, device='cuda')
+      keep.append(ptrs)
+      kw[l.name] = ptrs
       kw[f'{l.name}_extraOffset'] = l.extra_offset
   if flags is not None:
     kw['flags'] = torch.tensor(flags, dtype=torch.int32, device='cuda')
@@ -41,7 +50,7 @@ def _run(case, precision, n, seed=3, dist='uniform', use_flags=False, variant=No
   assert errf(None) == 0
   # oracle on float32-exact inputs
   multilinear.evaluate(descrs, mem, n, flags=flags)
-  out = [l for l in lay if l.kind == 'strided' and l.tensor.direction.name != 'SOURCE'][0]
+  out = [l for l in lay if l.kind in ('strided', 'ptr') and l.tensor.direction.name != 'SOURCE'][0]
   got = dev[out.name].double().cpu().numpy()
   ref = mem.buffers[out.name]
   return got, ref, out, flags
@@ -107,3 +116,12 @@ def test_chain_o6_per_term_pipeline(precision):
   got, ref, _, _ = _run('chain_o6', precision, 1333, variant={'pipe': 1})
   rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
   assert rel <= TOL[precision], rel
+
+
+@pytest.mark.parametrize('case', ['c0_gemm_ptr', 'c0_gemm_strided', 'gemm_add', 'chain_o3_dense', 'sparse_a_shared'])
+def test_other_chains_on_tensor_cores(case):
+  """Pointer arrays (cp.async staging, per-lane output stores), accumulation into the
+  output, a term without R, dense and sparse shared operands, all at TF32x3."""
+  got, ref, _, _ = _run(case, 'tf32x3', 203)
+  rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+  assert rel <= 1e-6, rel
