@@ -6,7 +6,8 @@ variants that the planner realises identically (a constant-memory A that falls b
 shared memory, a column program that does not fit and falls back to the generic plan) are
 kept once. `build_chain` is pure host work and returns a picklable `ChainBuild`, so a
 process pool can compile while the GPU process measures. Timings are cached per (GPU
-name, chain signature) as JSON, so interrupted tuning runs resume where they stopped.
+name and driver, variant space, chain signature) as JSON, so interrupted tuning runs resume
+where they stopped.
 """
 import hashlib
 import json
@@ -140,8 +141,9 @@ def is_cached(cache, spec, gpu):
 
 
 def _cache_path(cache, spec, gpu):
+  from .variants import space_signature
   h = hashlib.sha1(spec.key().encode()).hexdigest()[:16]
-  return os.path.join(cache, gpu, f'{h}.json')
+  return os.path.join(cache, gpu, f'space_{space_signature()}', f'{h}.json')
 
 
 def measure_chain(cb: ChainBuild, cache=None, reps=3, warmup=1, check_tol=1e-3, slow_ms=100.0):

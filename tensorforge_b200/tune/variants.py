@@ -4,7 +4,7 @@ import math
 from ..plan import SMEM_LIMIT
 from ..plan.chains import match_left_chain
 
-GENERIC_G = (4, 8, 16, 32, 64)
+GENERIC_G = (4, 8, 16, 32, 64, 128, 256)
 GENERIC_E = (1, 2, 4, 8, 16)
 COLPROG = [dict(threads=t, a_source=a) for t in (128, 256) for a in ("const", "smem")]
 NFEAT = 32
@@ -96,3 +96,10 @@ def features(chain, variant, batch):
 def effective_variant(plan):
   """The variant dict a plan realises (its strategy and applied parameters)."""
   return dict(strategy=plan.strategy, **plan.params)
+
+
+def space_signature():
+  """Short hash of the variant space: tuning results are only comparable within one space."""
+  import hashlib
+  key = repr((GENERIC_G, GENERIC_E, COLPROG, TUNE_COLPROG_MAX_FMAS, NFEAT))
+  return hashlib.sha1(key.encode()).hexdigest()[:8]
