@@ -104,6 +104,23 @@ class Memory:
     self.scalars = {}
 
 
+def _stored_targets(d):
+  """Per operand, the index of each *stored* dimension: target[i][v] names view dimension v,
+  which is stored dimension permute[i][v] (descriptions.py:126-149 expresses GEMM
+  transposes this way; the reference generator stops with NameError on such permutes)."""
+  out = []
+  for i, tgt in enumerate(d.target):
+    perm = d.permute[i] if d.permute is not None and i < len(d.permute) else None
+    if not perm or len(perm) != len(tgt) or sorted(perm) != list(range(len(tgt))):
+      out.append(list(tgt))
+      continue
+    eff = [0] * len(tgt)
+    for v, sdim in enumerate(perm):
+      eff[sdim] = tgt[v]
+    out.append(eff)
+  return out
+
+
 def evaluate(descr_list, memory: Memory, num_elements: int, flags=None, quirks=True):
   """Run the chain on every allowed element, updating memory.buffers in place."""
   tensors, symbols = name_operands(descr_list)
@@ -124,9 +141,10 @@ def evaluate(descr_list, memory: Memory, num_elements: int, flags=None, quirks=T
   tmp_values = {}   # id(tensor) -> (ranges, array [ne, *sizes])
 
   for d in descr_list:
+    targets = _stored_targets(d)
     # index ranges
     nr, kr = {}, {}
-    for sub, tgt in zip(d.ops, d.target):
+    for sub, tgt in zip(d.ops, targets):
       for j, t in enumerate(tgt):
         lo, up = sub.bbox.lower()[j], sub.bbox.upper()[j]
         table, key = (nr, t) if t >= 0 else (kr, -t - 1)
@@ -140,7 +158,7 @@ def evaluate(descr_list, memory: Memory, num_elements: int, flags=None, quirks=T
     letters_k = 'pqrstuvw'
 
     operands, subs = [], []
-    for i_op, (sub, tgt) in enumerate(zip(d.ops, d.target)):
+    for i_op, (sub, tgt) in enumerate(zip(d.ops, targets)):
       t = sub.tensor
       box = [n_ranges[x] if x >= 0 else k_ranges[-x - 1] for x in tgt]
       sizes = [u - l for l, u in box]

@@ -120,6 +120,28 @@ class Stage:
     return 2 * count_products(self)
 
 
+def stored_targets(descr):
+  """Targets per operand in the operand's stored dimension order.
+
+  `target[i][d]` names the index of dimension d of operand i *as permuted by*
+  `permute[i]` (view dimension d is stored dimension permute[i][d]), which is how
+  GemmDescr expresses transposes (descriptions.py:126-149: trans_a -> permute [1, 0] with
+  target [0, -1]). The reference itself stops with NameError for any non-identity
+  permute, so this is the intent of its interface rather than observed behaviour.
+  """
+  out = []
+  for i, tgt in enumerate(descr.target):
+    perm = descr.permute[i] if descr.permute is not None and i < len(descr.permute) else None
+    if not perm or len(perm) != len(tgt) or sorted(perm) != list(range(len(tgt))):
+      out.append(list(tgt))
+      continue
+    eff = [0] * len(tgt)
+    for view_dim, stored_dim in enumerate(perm):
+      eff[stored_dim] = tgt[view_dim]
+    out.append(eff)
+  return out
+
+
 def count_products(stage: Stage) -> int:
   """Number of nonzero scalar products of one stage (used for nz-FLOP rooflines)."""
   if stage.is_matmul():
@@ -262,7 +284,7 @@ def lower(descr_list, matrix_list, global_symbols, fp: FloatingPointType) -> Cha
     refs = []
     nr: Dict[int, Tuple[int, int]] = {}
     kr: Dict[int, Tuple[int, int]] = {}
-    for sub, tgt in zip(d.ops, d.target):
+    for sub, tgt in zip(d.ops, stored_targets(d)):
       o = ops_by_tensor[id(sub.tensor)]
       refs.append(OpRef(o, sub.bbox, list(tgt)))
       for j, t in enumerate(tgt):
@@ -293,10 +315,18 @@ def lower(descr_list, matrix_list, global_symbols, fp: FloatingPointType) -> Cha
       raise GenerationError('a scalar or compile-time tensor cannot be written')
     if len(n_ranges) != len(dest.shape) and dest.kind != 'tmp':
       raise GenerationError(f'result rank {len(n_ranges)} does not match {dest}')
+    if dest.kind != 'tmp':
+      # the result is stored relative to the destination box's lower corner: every stored
+      # index must stay inside the destination's shape (else it would land in another
+      # element's data or past the buffer)
+      for t, (lo, up) in enumerate(n_ranges):
+        base = d.dest.bbox.lower()[t]
+        if lo - base < 0 or up - base > dest.shape[t]:
+          raise GenerationError(f'result index range n{t} [{lo}, {up}) of {d} does not fit the '
+                                f'destination (box from {base}, extent {dest.shape[t]})')
     st = Stage(dest, d.dest.bbox, refs, bool(d.add), n_ranges, k_ranges, descr=d)
-    # permute changes nothing semantically, but the reference reads a non-permuted,
-    # lead-less dense operand through a compact copy of its bounding box (load.py:76-137);
-    # both layouts coincide when the bounding box covers the whole shape.
+    # the reference reads a non-permuted, lead-less dense operand through a compact copy of
+    # its bounding box (load.py:76-137); both layouts coincide when the box covers the shape.
     for idx_op, ref in enumerate(st.ops):
       o = ref.op
       dsc_perm = d.permute[idx_op] if idx_op < len(d.permute) else list(range(len(ref.target)))

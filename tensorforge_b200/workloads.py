@@ -98,6 +98,18 @@ def subbox_gemm(ns, box_a, box_b, box_c, shape=56, addr='strided', trans_a=False
   return [ns.GemmDescr(trans_a, trans_b, ns.SubTensor(A), ns.SubTensor(B), ns.SubTensor(C))]
 
 
+def suite_gemm(ns, a, b, c, trans_a=False, trans_b=False, alpha=1.0):
+  """One GEMM of the reference's YAML test suites (tests/gemms/testsuites/*.yaml): each of
+  a, b, c is {'rows', 'cols', 'addressing', 'bbox': [r0, c0, r1, c1]} in stored order."""
+  BB = ns.BoundingBox
+
+  def tensor(m):
+    box = m['bbox']
+    return ns.Tensor([m['rows'], m['cols']], ns.Addressing.str2addr(m['addressing']), BB(box[:2], box[2:]))
+  A, B, C = tensor(a), tensor(b), tensor(c)
+  return [ns.GemmDescr(trans_a, trans_b, ns.SubTensor(A), ns.SubTensor(B), ns.SubTensor(C), alpha=alpha)]
+
+
 def three_matrices(ns):
   """D += A x (B x C) with a temporary (example/three_matrices.py:9-32)."""
   BB = ns.BoundingBox
