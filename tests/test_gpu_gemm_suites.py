@@ -37,6 +37,7 @@ def test_suite_case_matches_oracle(case):
   dev, kw = {}, {'numElements': n}
   for l in lay:
     if l.kind == 'scalar':
+      kw[l.name] = mem.scalars[l.name]
       continue
     dev[l.name] = torch.tensor(mem.buffers[l.name], dtype=torch.float32, device='cuda')
     kw[l.name] = dev[l.name]
