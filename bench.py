@@ -337,6 +337,35 @@ def extra_workloads(stream, short=False):
     del kw
   out['c2_precision_loguniform'] = {'elements': n2, 'values': 'sign * 10^U(-3,3), seed 7', 'variants': c2}
   torch.cuda.empty_cache()
+  # elementwise stage: pointwise nonlinear update of a 56x9 block per element (HBM bound)
+  from tensorforge_b200.kernels import EW_BENCH_VARIANTS
+  from tensorforge_b200.common.basic_types import FloatingPointType
+  from tensorforge_b200.common.context import Context, Options
+  from tensorforge_b200.generators.generator import Generator
+  ns = cases.ns_from_module('tensorforge_b200')
+  n = 200000 if short else 1000000
+  hbm = peaks()[0]['hbm_gbs']
+  ew = {}
+  bufs = {}
+  for v in [None] + EW_BENCH_VARIANTS:
+    g = Generator(cases.build_elementwise('ew_update', ns), Context('sm_100a', 'cuda', FloatingPointType.FLOAT,
+                                                                    Options(variant=v)))
+    g.generate()
+    k = compile_generator(g)
+    if not bufs:
+      for t, _ in g.abi_symbols():
+        bufs[t.name] = 0.5 if t.addressing.name == 'SCALAR' else torch.rand(n * t.get_real_volume(), device=dev) * 2 - 1
+    kw = dict(bufs, numElements=n)
+    total, per = time_launches(lambda: k(**kw), stream, 5, 2)
+    ms = sum(per) / len(per)
+    gbs = n * g.get_chain().bytes_per_element() / (ms / 1e3) / 1e9
+    ew['default' if v is None else g.get_plan().key()] = {
+      'elements_per_s': n / (ms / 1e3), 'ms': ms, 'hbm_gbs': gbs, 'frac_hbm': gbs / hbm, 'plan': g.get_plan().key()}
+  out['elementwise_update'] = {'elements': n, 'bytes_per_element': 2 * 504 * 4, 'peak_hbm_gbs': hbm,
+                               'statements': 't = Q*s; O = t > 0 ? t*exp(-t*t) : 0.5*t (56x9, FP32)',
+                               'variants': ew}
+  bufs.clear()
+  torch.cuda.empty_cache()
   # FP64 order-6 chain
   n = 100000 if short else 500000
   for label, opts in (('fp64_colprog', {'variant': {'strategy': 'colprog'}}), ('fp64_dmma', {})):

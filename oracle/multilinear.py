@@ -45,7 +45,7 @@ def name_operands(descr_list):
   """
   seen = {}
   for d in descr_list:
-    for sub in [d.dest] + list(d.ops):
+    for sub in (d.matrix_list() if hasattr(d, 'oplist') else [d.dest] + list(d.ops)):
       seen.setdefault(id(sub.tensor), sub.tensor)
   tensors = list(seen.values())
   symbols = []
@@ -121,8 +121,11 @@ def _stored_targets(d):
   return out
 
 
-def evaluate(descr_list, memory: Memory, num_elements: int, flags=None, quirks=True):
-  """Run the chain on every allowed element, updating memory.buffers in place."""
+def evaluate(descr_list, memory: Memory, num_elements: int, flags=None, quirks=True, fp32=False):
+  """Run the chain on every allowed element, updating memory.buffers in place.
+
+  Elementwise descriptors run through oracle/elementwise.py (`fp32` applies to them).
+  """
   tensors, symbols = name_operands(descr_list)
   sym_names = {}
   for i, t in enumerate(symbols):
@@ -141,6 +144,10 @@ def evaluate(descr_list, memory: Memory, num_elements: int, flags=None, quirks=T
   tmp_values = {}   # id(tensor) -> (ranges, array [ne, *sizes])
 
   for d in descr_list:
+    if hasattr(d, 'oplist'):
+      from .elementwise import evaluate_elementwise
+      evaluate_elementwise(d, memory, elems, sym_names, tmp_values, fp32=fp32)
+      continue
     targets = _stored_targets(d)
     # index ranges
     nr, kr = {}, {}

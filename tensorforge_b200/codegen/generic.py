@@ -13,6 +13,7 @@ from functools import reduce
 
 from ..common.basic_types import FloatingPointType
 from ..common.exceptions import GenerationError
+from .elementwise import emit_elementwise_stage
 
 
 def _prod(xs):
@@ -44,11 +45,7 @@ def smem_layout(chain):
     if o.kind == 'batched' and o.sparse:
       per_elem += _prod(_sparse_box(o))
   for t in chain.tmps:
-    best = 0
-    for s in chain.stages:
-      if s.dest is t:
-        best = max(best, s.out_volume())
-    per_elem += best
+    per_elem += max([s.defines_volume(t) for s in chain.stages] + [0])
   # keep every region 16-byte aligned for vector accesses
   return _align4(shared), _align4(per_elem)
 
@@ -104,7 +101,7 @@ class GenericEmitter:
         regions[o.name] = ('elem', off, _sparse_box(o))
         off += _prod(_sparse_box(o))
     for t in self.chain.tmps:
-      vol = max([s.out_volume() for s in self.chain.stages if s.dest is t] + [0])
+      vol = max([s.defines_volume(t) for s in self.chain.stages] + [0])
       regions[t.name] = ('elem', off, None)
       off += vol
     per_elem = _align4(off)
@@ -247,7 +244,10 @@ class GenericEmitter:
       for si, st in enumerate(chain.stages):
         self.w(f'// stage {si}: {st.descr}'.replace('\n', ' '))
         with self.block('if (active)'):
-          self._emit_stage(st, regions)
+          if getattr(st, 'kind', '') == 'elementwise':
+            emit_elementwise_stage(self, st)
+          else:
+            self._emit_stage(st, regions)
         self.w(f'{sync};')
     self.ind -= 1
     self.w('}')

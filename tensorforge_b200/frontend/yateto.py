@@ -20,7 +20,7 @@ from ..common.exceptions import GenerationError
 from ..common.matrix.tensor import Tensor, SubTensor
 from ..common.matrix.spp import FullSPP, ListSPP
 from ..common.matrix.boundingbox import BoundingBox
-from ..generators.descriptions import MultilinearDescr
+from ..generators.descriptions import MultilinearDescr, ElementwiseDescr
 from ..generators.generator import Generator
 from ..interface import YatetoInterface
 
@@ -134,6 +134,44 @@ class GpuKernelGeneratorV1:
       self._cache[dest.name] = self._tmp[dest.name]
     else:
       self._make(dest)
+
+  def _name(self, op):
+    return op.name() if self._is_scalar(op) else op.name
+
+  def add_scalar(self, ops, statements, indices):
+    """Elementwise statements over yateto tensors (frontend/yateto.py:127-149).
+
+    `statements` are optree statements whose tensor variables were made from the yateto
+    nodes in `ops`; `indices[i]` is the index list of ops[i] (-1 for n0, -2 for n1, ...).
+    Scalars take no indices. A temporary that the statements write before anything
+    produced it becomes a new strided temporary with the layout's shape.
+    """
+    index_of = {}
+    for op, idx in zip(ops, indices):
+      if isinstance(op, (float, int)):
+        continue
+      if getattr(op, 'is_temporary', False) and op.name not in self._tmp:
+        tml = self._storage(op.memoryLayout)
+        rng = tml.bbox()
+        t = Tensor([r.stop for r in rng], Addressing.STRIDED,
+                   BoundingBox([r.start for r in rng], [r.stop for r in rng]), op.name, True)
+        self._tmp[op.name] = t
+      self._make(op)
+      index_of[self._name(op)] = [] if self._is_scalar(op) else list(idx)
+
+    def assigner(pre):
+      if self._is_scalar(pre):
+        self._make(pre)
+        index_of.setdefault(pre.name(), [])
+      name = self._name(pre)
+      if name not in index_of:
+        raise GenerationError(f'{name} is used by the statements but not listed in ops')
+      return self._sub(pre), index_of[name]
+
+    for st in statements:
+      st.assignTensor(assigner)
+    self._descr_list.append(ElementwiseDescr(statements))
+    return 0
 
   # ------------------------------------------------------------------ dictionary API
   def add_tensor(self, d):

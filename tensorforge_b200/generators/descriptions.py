@@ -6,8 +6,11 @@
 
 where `target[i][j] >= 0` maps dimension j of operand i to output index n_t and
 `target[i][j] < 0` maps it to the contracted index k_{-t-1}. Index ranges are the
-intersections of the operands' bounding boxes. `permute` is carried for interface
-compatibility; like the reference it does not change which entries are multiplied.
+intersections of the operands' bounding boxes. `permute[i][d]` is the stored dimension
+of operand i that `target[i][d]` indexes (how `GemmDescr` expresses transposes).
+
+`ElementwiseDescr(statements)` describes pointwise statements (see `optree`) over an
+index box; both kinds can be mixed in one descriptor list.
 """
 from typing import List
 from ..common.exceptions import GenerationError
@@ -94,9 +97,41 @@ class GemmDescr(MultilinearDescr):
 
 
 class ElementwiseDescr(OperationDescription):
-  """Placeholder for elementwise statements (descriptions.py:67-95); not lowered by this generator."""
+  """Elementwise statements over an index box, per batch element (descriptions.py:67-95).
+
+  `oplist` holds `optree` statements (`Assignment`, `IfNode`, `WhileNode`) whose tensor
+  variables are bound. Tensors assigned to become SINK, tensors read become SOURCE (both:
+  SOURCESINK), as in the reference. Stages of this kind can be mixed with
+  `MultilinearDescr`s in one descriptor list: they read and write batched operands and
+  temporaries, and a temporary written here can feed a later contraction.
+  """
 
   def __init__(self, oplist, strict_match: bool = False, prefer_align: bool = False):
-    self.oplist = oplist
+    from .optree import Statement, label_temporaries
+    self.oplist = list(oplist)
     self._strict_match = False
-    raise GenerationError('elementwise statements are not supported by the sm_100a generator')
+    for op in self.oplist:
+      if not isinstance(op, Statement):
+        raise GenerationError(f'elementwise statements must be optree statements, got {type(op).__name__}')
+    for op in self.oplist:
+      for sub in op.tensors(outtensors=True, intensors=False):
+        sub.tensor.set_data_flow_direction(DataFlowDirection.SINK)
+    for op in self.oplist:
+      for sub in op.tensors(outtensors=False, intensors=True):
+        sub.tensor.set_data_flow_direction(DataFlowDirection.SOURCE)
+    label_temporaries(self.oplist)
+
+  def get_num_threads(self, context):
+    return 64, 64
+
+  def get_accumulator_size(self):
+    return 0
+
+  def is_strict_match(self):
+    return self._strict_match
+
+  def matrix_list(self):
+    return [sub for op in self.oplist for sub in op.tensors()]
+
+  def __str__(self):
+    return '; '.join(str(op) for op in self.oplist)

@@ -16,7 +16,7 @@ from ..common.basic_types import Addressing, GeneralLexicon, DataFlowDirection
 from ..common.context import Context
 from ..common.exceptions import GenerationError
 from ..ir.chain import lower
-from .descriptions import OperationDescription, MultilinearDescr
+from .descriptions import OperationDescription, MultilinearDescr, ElementwiseDescr
 
 
 class RegmaxBlockPolicy:
@@ -45,7 +45,7 @@ class Generator:
     self._plan = None
     self._emitted = None
     for d in self.descr_list:
-      if not isinstance(d, MultilinearDescr):
+      if not isinstance(d, (MultilinearDescr, ElementwiseDescr)):
         raise GenerationError(f'unsupported operation description: {type(d).__name__}')
     self._check_consistency_with_user_options()
     self._name_operands(self.descr_list)

@@ -119,6 +119,19 @@ class Stage:
     """Multiply-adds counted over nonzero operand entries only, times 2."""
     return 2 * count_products(self)
 
+  def dense_flops(self):
+    return 2 * self.out_volume() * self.k_volume()
+
+  def touched_volume(self, o):
+    best = self.out_volume() if self.dest is o else 0
+    for r in self.ops:
+      if r.op is o:
+        best = max(best, _prod([u - l for l, u in _op_box(self, r)]))
+    return best
+
+  def defines_volume(self, o):
+    return self.out_volume() if self.dest is o else 0
+
 
 def stored_targets(descr):
   """Targets per operand in the operand's stored dimension order.
@@ -187,7 +200,10 @@ class Chain:
     return sum(s.nz_flops() for s in self.stages)
 
   def dense_flops_per_element(self):
-    return sum(2 * s.out_volume() * s.k_volume() for s in self.stages)
+    return sum(s.dense_flops() for s in self.stages)
+
+  def has_elementwise(self):
+    return any(getattr(s, 'kind', '') == 'elementwise' for s in self.stages)
 
   def bytes_per_element(self):
     """Algorithmic HBM bytes per element: every batched input read once, every output
@@ -209,13 +225,7 @@ class Chain:
 
 
 def _touched_volume(chain, o):
-  best = 0
-  for s in chain.stages:
-    if s.dest is o:
-      best = max(best, s.out_volume())
-    for r in s.ops:
-      if r.op is o:
-        best = max(best, _prod([u - l for l, u in _op_box(s, r)]))
+  best = max([s.touched_volume(o) for s in chain.stages] + [0])
   return best if best > 0 else o.tensor.get_actual_volume()
 
 
@@ -224,7 +234,8 @@ def _reads_dest(chain, o):
   for s in chain.stages:
     if any(r.op is o for r in s.ops):
       return True
-    if s.dest is o:
+    written = any(x is o for x in s.written) if getattr(s, 'kind', '') == 'elementwise' else (s.dest is o)
+    if written:
       if s.add and first:
         return True
       first = False
@@ -281,6 +292,10 @@ def lower(descr_list, matrix_list, global_symbols, fp: FloatingPointType) -> Cha
   stages = []
   tmp_ranges: Dict[int, List[Tuple[int, int]]] = {}
   for d in descr_list:
+    if hasattr(d, 'oplist'):
+      from .elementwise import lower_elementwise
+      stages.append(lower_elementwise(d, ops_by_tensor, tmp_ranges))
+      continue
     refs = []
     nr: Dict[int, Tuple[int, int]] = {}
     kr: Dict[int, Tuple[int, int]] = {}

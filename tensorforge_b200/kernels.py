@@ -69,6 +69,46 @@ def catalogue():
   return out
 
 
+EW_LAUNCH_SHAPES = [
+  {'strategy': 'generic', 'threads_per_element': 32, 'elements_per_block': 4},
+  {'strategy': 'generic', 'threads_per_element': 128, 'elements_per_block': 2},
+  {'strategy': 'generic', 'threads_per_element': 8, 'elements_per_block': 16},
+]
+
+
+def elementwise_catalogue():
+  """(name, Generator) for the elementwise workloads: both precisions, plus the launch
+  shapes the tests sweep and the benchmark's variants."""
+  from . import workloads
+  from .common.basic_types import FloatingPointType
+  from .common.context import Context, Options
+  from .generators.generator import Generator
+  ns = workloads.ns_from_module('tensorforge_b200')
+  out = []
+
+  def add(name, fp, variant=None):
+    ftype = FloatingPointType.FLOAT if fp == 'float' else FloatingPointType.DOUBLE
+    g = Generator(workloads.build_elementwise(name, ns), Context('sm_100a', 'cuda', ftype, Options(variant=variant)))
+    g.generate()
+    out.append((f'{name}/{fp}/{variant}', g))
+
+  for name in workloads.EW_CASES:
+    for fp in ('float', 'double'):
+      add(name, fp)
+  for v in EW_LAUNCH_SHAPES:
+    for name in ('ew_update', 'ew_feeds_contraction', 'ew_views'):
+      add(name, 'float', v)
+  for v in EW_BENCH_VARIANTS:
+    add('ew_update', 'float', v)
+  return out
+
+
+EW_BENCH_VARIANTS = [
+  {'strategy': 'generic', 'threads_per_element': g, 'elements_per_block': e}
+  for g, e in ((64, 1), (64, 4), (32, 8), (128, 2), (256, 1), (512, 1))
+]
+
+
 def grouped_catalogue():
   """Grouped (mixed-shape) kernels used by the tests and the benchmark."""
   from . import workloads as cases

@@ -46,6 +46,8 @@ def ns_from_module(root):
   ns.FloatingPointType = bt.FloatingPointType
   ns.MultilinearDescr, ns.GemmDescr = de.MultilinearDescr, de.GemmDescr
   ns.generate_tmp_tensor = ax.generate_tmp_tensor
+  ns.ElementwiseDescr = de.ElementwiseDescr
+  ns.optree = importlib.import_module(f'{root}.generators.optree')
   return ns
 
 
@@ -228,3 +230,154 @@ def mixed_chain(ns, basis, quantities, seed=0):
   """The order-`basis` volume chain with patterns seeded per shape (S density ~30%)."""
   nnz = max(1, int(round(0.3 * quantities * quantities)))
   return volume_chain(ns, basis=basis, quantities=quantities, s_nnz=nnz, seed=seed * 100 + basis * 7 + quantities)
+
+
+# --------------------------------------------------------------------------- elementwise
+# Statement programs over batched tensors (`ElementwiseDescr`), alone and fused with
+# contractions. Built with tensorforge_b200 only: the reference's optree binds tensor
+# variables through yateto, and its code generators do not emit elementwise stages.
+
+def ew_update(ns, rows=56, cols=9, addr='strided'):
+  """Pointwise nonlinear update of one 56x9 block per element, with a scalar gain:
+
+      t = Q * s;  O = t > 0 ? t * exp(-t * t) : 0.5 * t
+
+  One read and one write of the block: the HBM-bound elementwise workload."""
+  ot = ns.optree
+  a = ns.Addressing.str2addr(addr)
+  Q, O = ns.Tensor([rows, cols], a), ns.Tensor([rows, cols], a)
+  s = ns.Tensor([], ns.Addressing.SCALAR)
+  t = ot.temp()
+  return [ns.ElementwiseDescr([
+    ot.assign(t, ot.tensor(Q) * ot.scalar(s)),
+    ot.assign(ot.tensor(O), ot.ternary(t > 0.0, t * ot.exp(-(t * t)), 0.5 * t)),
+  ])]
+
+
+EW_FUNCTIONS = [
+  # (name, expression builder over x in [-1, 1]) -- arguments kept inside each domain
+  ('exp', lambda ot, x: ot.exp(x)), ('log', lambda ot, x: ot.log(ot.abs(x) + 0.5)),
+  ('expm1', lambda ot, x: ot.expm1(x)), ('logp1', lambda ot, x: ot.logp1(ot.abs(x))),
+  ('sqrt', lambda ot, x: ot.sqrt(ot.abs(x))), ('cbrt', lambda ot, x: ot.cbrt(x)),
+  ('rsqrt', lambda ot, x: ot.rsqrt(ot.abs(x) + 0.25)),
+  ('rcbrt', lambda ot, x: ot.rcbrt(x + 2.0)), ('pow', lambda ot, x: ot.pow(ot.abs(x) + 0.5, 1.3)),
+  ('sin', lambda ot, x: ot.sin(3.0 * x)), ('cos', lambda ot, x: ot.cos(3.0 * x)),
+  ('tan', lambda ot, x: ot.tan(x)), ('asin', lambda ot, x: ot.asin(0.9 * x)),
+  ('acos', lambda ot, x: ot.acos(0.9 * x)), ('atan', lambda ot, x: ot.atan(4.0 * x)),
+  ('sinh', lambda ot, x: ot.sinh(2.0 * x)), ('cosh', lambda ot, x: ot.cosh(2.0 * x)),
+  ('tanh', lambda ot, x: ot.tanh(2.0 * x)), ('asinh', lambda ot, x: ot.asinh(3.0 * x)),
+  ('acosh', lambda ot, x: ot.acosh(ot.abs(x) + 1.5)), ('atanh', lambda ot, x: ot.atanh(0.9 * x)),
+  ('erf', lambda ot, x: ot.erf(2.0 * x)), ('gamma', lambda ot, x: ot.gamma(x + 2.0)),
+  ('abs', lambda ot, x: abs(x)), ('neg', lambda ot, x: -x), ('rcp', lambda ot, x: 1.0 / (x + 2.0)),
+  ('ceil', lambda ot, x: ot.ceil(4.0 * x)), ('floor', lambda ot, x: ot.floor(4.0 * x)),
+  ('round', lambda ot, x: ot.round(4.0 * x)), ('trunc', lambda ot, x: ot.trunc(4.0 * x)),
+  ('sign', lambda ot, x: ot.sign(x)), ('mod', lambda ot, x: (8.0 * x) % 3.0),
+  ('min', lambda ot, x: ot.min(x, 0.25)), ('max', lambda ot, x: ot.max(x, -0.25)),
+  ('square', lambda ot, x: x ** 2), ('div', lambda ot, x: x / (x * x + 1.0)),
+]
+
+
+def ew_functions(ns, rows=12, cols=5):
+  """One stage per operation, each writing its own slice O[:, :, f] of a rank-3 output
+  (a view with a nonzero box corner in the last dimension)."""
+  ot = ns.optree
+  Q = ns.Tensor([rows, cols], ns.Addressing.STRIDED)
+  O = ns.Tensor([rows, cols, len(EW_FUNCTIONS)], ns.Addressing.STRIDED)
+  out = []
+  for f, (_, fn) in enumerate(EW_FUNCTIONS):
+    view = ns.SubTensor(O, ns.BoundingBox([0, 0, f], [rows, cols, f + 1]))
+    out.append(ns.ElementwiseDescr([ot.assign(ot.tensor(view), fn(ot, ot.tensor(Q)))]))
+  return out
+
+
+def ew_control(ns, rows=20, cols=7):
+  """Temporaries, if, ternary, a while loop with an integer counter, casts and integer /
+  boolean operators: Newton's iteration for sqrt(x^2 + 1) plus branch-dependent terms."""
+  ot = ns.optree
+  FP = ns.FloatingPointType
+  Q = ns.Tensor([rows, cols], ns.Addressing.PTR_BASED)
+  P = ns.Tensor([rows, cols], ns.Addressing.STRIDED)
+  O = ns.Tensor([rows, cols], ns.Addressing.STRIDED)
+  x, y, i, flag = ot.temp(), ot.temp(), ot.temp(FP.INT), ot.temp(FP.BOOL)
+  q, p, o = ot.tensor(Q), ot.tensor(P), ot.tensor(O)
+  return [ns.ElementwiseDescr([
+    ot.assign(x, q * q + 1.0),
+    ot.assign(y, x),
+    ot.loop(i < 6, [ot.assign(y, 0.5 * (y + x / y)), ot.assign(i, i + 1)]),
+    ot.assign(flag, (q > 0.0) & ~(p < -0.5)),
+    ot.assign(o, y),
+    ot.conditional(flag, [ot.assign(o, o + p)]),
+    ot.conditional((q < 0.0) | (p > 0.5), [ot.assign(o, o - ot.cast(ot.cast(4.0 * p, FP.INT) % 3, FP.FLOAT) * 0.125)]),
+    ot.assign(o, o + ot.ternary(ot.bitxor(q > 0.0, p > 0.0), 2.0, ot.cast(i & 3, FP.FLOAT))),
+  ])]
+
+
+def ew_fused_chain(ns, basis=20, quantities=9):
+  """A contraction into a temporary followed by an elementwise stage that accumulates a
+  rectified copy into the output: T = K * Q;  O = O + max(T, 0) * s."""
+  ot = ns.optree
+  K = ns.Tensor([basis, basis], ns.Addressing.NONE)
+  Q = ns.Tensor([basis, quantities], ns.Addressing.STRIDED)
+  O = ns.Tensor([basis, quantities], ns.Addressing.PTR_BASED)
+  s = ns.Tensor([], ns.Addressing.SCALAR)
+  T = ns.generate_tmp_tensor([ns.SubTensor(K), ns.SubTensor(Q)], [[0, -1], [-1, 1]])
+  o = ot.tensor(O)
+  return [
+    ns.MultilinearDescr(ns.SubTensor(T), [ns.SubTensor(K), ns.SubTensor(Q)], [[0, -1], [-1, 1]], [[0, 1], [0, 1]]),
+    ns.ElementwiseDescr([ot.assign(o, o + ot.max(ot.tensor(T), 0.0) * ot.scalar(s))]),
+  ]
+
+
+def ew_feeds_contraction(ns, basis=16, quantities=9):
+  """An elementwise stage defines a temporary that a contraction consumes:
+  T = tanh(Q);  O = K * T;  O = O * O."""
+  ot = ns.optree
+  K = ns.Tensor([basis, basis], ns.Addressing.NONE)
+  Q = ns.Tensor([basis, quantities], ns.Addressing.STRIDED)
+  O = ns.Tensor([basis, quantities], ns.Addressing.STRIDED)
+  T = ns.Tensor([basis, quantities], ns.Addressing.STRIDED, is_tmp=True)
+  return [
+    ns.ElementwiseDescr([ot.assign(ot.tensor(T), ot.tanh(ot.tensor(Q)))]),
+    ns.MultilinearDescr(ns.SubTensor(O), [ns.SubTensor(K), ns.SubTensor(T)], [[0, -1], [-1, 1]], [[0, 1], [0, 1]]),
+    ns.ElementwiseDescr([ot.assign(ot.tensor(O), ot.tensor(O) ** 2)]),
+  ]
+
+
+def ew_views(ns):
+  """Sub-box views and a transposed read: O[2+n0, 1+n1] = Q[3+n1, 4+n0] * 2 + B[n0, n1]
+  with a 6x5 index box."""
+  ot = ns.optree
+  Q = ns.Tensor([10, 12], ns.Addressing.STRIDED)
+  B = ns.Tensor([6, 5], ns.Addressing.NONE)
+  O = ns.Tensor([9, 8], ns.Addressing.STRIDED)
+  qv = ns.SubTensor(Q, ns.BoundingBox([3, 4], [8, 10]))
+  ov = ns.SubTensor(O, ns.BoundingBox([2, 1], [8, 6]))
+  return [ns.ElementwiseDescr([
+    ot.assign(ot.tensor(ov), ot.tensor(qv, indices=[-2, -1]) * 2.0 + ot.tensor(B)),
+  ])]
+
+
+def ew_sparse_read(ns, rows=14, cols=9, seed=4):
+  """A compactly stored sparse operand read pointwise (absent entries read 0):
+  O = 2 * S + 1."""
+  ot = ns.optree
+  S = ns.Tensor([rows, cols], ns.Addressing.STRIDED, spp=ns.ListSPP(sparse_pattern(rows, cols, 0.4, seed), [rows, cols]))
+  O = ns.Tensor([rows, cols], ns.Addressing.STRIDED)
+  return [ns.ElementwiseDescr([ot.assign(ot.tensor(O), 2.0 * ot.tensor(S) + 1.0)])]
+
+
+EW_CASES = {
+  # name: (builder, kwargs, num_elements)
+  'ew_update': (ew_update, {}, 37),
+  'ew_functions': (ew_functions, {}, 9),
+  'ew_control': (ew_control, {}, 21),
+  'ew_fused_chain': (ew_fused_chain, {}, 19),
+  'ew_feeds_contraction': (ew_feeds_contraction, {}, 11),
+  'ew_views': (ew_views, {}, 7),
+  'ew_sparse_read': (ew_sparse_read, {}, 13),
+}
+
+
+def build_elementwise(name, ns):
+  fn, kwargs, _ = EW_CASES[name]
+  return fn(ns, **kwargs)
