@@ -30,12 +30,13 @@ def _colmajor(sizes):
 class PointEmitter:
   """Emits the body of one point of an elementwise stage into a GenericEmitter."""
 
-  def __init__(self, em, stage):
+  def __init__(self, em, stage, sfx='', counter=None):
     self.em = em
     self.stage = stage
     self.fp = em.ctx.fp_type
     self.T = em.T
-    self.count = 0
+    self.sfx = sfx                      # name suffix of this point's indices and temporaries
+    self.counter = counter if counter is not None else [0]
     self.memo = {}
 
   # ------------------------------------------------------------------ types
@@ -50,7 +51,7 @@ class PointEmitter:
 
   # ------------------------------------------------------------------ operands
   def _index_exprs(self, acc):
-    return [f'(n{d} + {b})' for d, b in zip(acc.dims, acc.base)]
+    return [f'(n{d}{self.sfx} + {b})' for d, b in zip(acc.dims, acc.base)]
 
   def _address(self, acc):
     terms = [f'({e} - {org}) * {st}' for e, org, st in zip(self._index_exprs(acc), acc.origin, acc.strides)]
@@ -90,8 +91,8 @@ class PointEmitter:
     return out
 
   def _local(self, ty, text):
-    name = f'e{self.count}'
-    self.count += 1
+    name = f'e{self.counter[0]}'
+    self.counter[0] += 1
     self.em.w(f'const {self.ctype(ty)} {name} = {text};')
     return name
 
@@ -103,7 +104,7 @@ class PointEmitter:
         return f'{int(node.value)}', 'int'
       return self.em.lit(node.value), 'fp'
     if isinstance(node, ot.TempVar):
-      return node.label, self._temp_type(node)
+      return node.label + self.sfx, self._temp_type(node)
     if isinstance(node, (ot.TensorVar, ot.ScalarVar)):
       return self._local('fp', self.load(node)), 'fp'
     if isinstance(node, ot.ConditionalOpNode):
@@ -189,26 +190,28 @@ class PointEmitter:
     for t in self.stage.temporaries():
       ty = self._temp_type(t)
       zero = {'fp': self.em.lit(0.0), 'int': '0', 'bool': 'false'}.get(ty, '0')
-      self.em.w(f'{self.ctype(ty)} {t.label} = {zero};')
+      self.em.w(f'{self.ctype(ty)} {t.label}{self.sfx} = {zero};')
+
+  def store(self, s, v, vt):
+    if isinstance(s.dest, ot.TempVar):
+      ty = self._temp_type(s.dest)
+      val = self._fp(v, vt) if ty == 'fp' else f'static_cast<{self.ctype(ty)}>({v})'
+      self.em.w(f'{s.dest.label}{self.sfx} = {val};')
+    else:
+      self.em.w(f'{self.lvalue(s.dest)} = {self._fp(v, vt)};')
 
   def statements(self, stmts, depth=0):
     for s in stmts:
       self.memo = {}  # values are re-read after every statement (it may have stored to them)
       if isinstance(s, ot.Assignment):
-        v, vt = self.expr(s.optree)
-        if isinstance(s.dest, ot.TempVar):
-          ty = self._temp_type(s.dest)
-          val = self._fp(v, vt) if ty == 'fp' else f'static_cast<{self.ctype(ty)}>({v})'
-          self.em.w(f'{s.dest.label} = {val};')
-        else:
-          self.em.w(f'{self.lvalue(s.dest)} = {self._fp(v, vt)};')
+        self.store(s, *self.expr(s.optree))
       elif isinstance(s, ot.IfNode):
         with self.em.block(''):
           c, _ = self.expr(s.condition)
           with self.em.block(f'if ({c})'):
             self.statements(s.subassignments, depth + 1)
       elif isinstance(s, ot.WhileNode):
-        g = f'w{depth}'
+        g = f'w{depth}{self.sfx}'
         with self.em.block(f'for (unsigned {g} = 0; {g} < {WHILE_LIMIT}u; ++{g})'):
           c, _ = self.expr(s.condition)
           self.em.w(f'if (!({c})) break;')
@@ -218,19 +221,62 @@ class PointEmitter:
       self.memo = {}
 
 
+def multi_point_statements(em, pes, stmts):
+  """Statements for several points at once, statement by statement: all points' values
+  (their loads in flight together) before any point's store. Points never touch each
+  other's entries (checked at lowering), so this order computes what running the points
+  one after another computes. `if` and `while` bodies run point by point."""
+  for s in stmts:
+    for pe in pes:
+      pe.memo = {}
+    if isinstance(s, ot.Assignment):
+      vals = [pe.expr(s.optree) for pe in pes]
+      for pe, (v, vt) in zip(pes, vals):
+        pe.store(s, v, vt)
+    elif isinstance(s, ot.IfNode):
+      conds = [pe.expr(s.condition)[0] for pe in pes]
+      for pe, c in zip(pes, conds):
+        with em.block(f'if ({c})'):
+          pe.statements(s.subassignments, 1)
+    else:
+      for pe in pes:
+        pe.statements([s])
+    for pe in pes:
+      pe.memo = {}
+
+
 def emit_elementwise_stage(em, stage):
-  """Point loop of one elementwise stage (inside the element's `if (active)`)."""
+  """Point loop of one elementwise stage (inside the element's `if (active)`).
+
+  The lanes of the group take points d = lane, lane + G, ...; a pass handles
+  `points_per_lane` (U) points per lane at once, then single points finish the rest."""
   G = em.G
+  U = int(em.plan.params.get('points_per_lane', 4))
   sizes = stage.sizes
   vol = 1
   for s in sizes:
     vol *= s
-  with em.block(f'for (unsigned d = lane; d < {vol}u; d += {G}u)'):
+  counter = [0]
+
+  def indices(d, sfx):
     div = 1
     for i, s in enumerate(sizes):
-      expr = f'(d / {div}u) % {s}u' if div > 1 else f'd % {s}u'
-      em.w(f'const int n{i} = (int)({expr});')
+      expr = f'({d} / {div}u) % {s}u' if div > 1 else f'{d} % {s}u'
+      em.w(f'const int n{i}{sfx} = (int)({expr});')
       div *= s
-    pe = PointEmitter(em, stage)
+
+  em.w('unsigned d0 = lane;')
+  if U > 1 and vol > G:
+    with em.block(f'for (; d0 + {(U - 1) * G}u < {vol}u; d0 += {U * G}u)'):
+      pes = []
+      for u in range(U):
+        indices(f'(d0 + {u * G}u)', f'_{u}')
+        pe = PointEmitter(em, stage, f'_{u}', counter)
+        pe.declare_temporaries()
+        pes.append(pe)
+      multi_point_statements(em, pes, stage.statements)
+  with em.block(f'for (; d0 < {vol}u; d0 += {G}u)'):
+    indices('d0', '')
+    pe = PointEmitter(em, stage, '', counter)
     pe.declare_temporaries()
     pe.statements(stage.statements)

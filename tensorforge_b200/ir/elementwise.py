@@ -201,9 +201,12 @@ def lower_elementwise(descr, ops_by_tensor, tmp_ranges) -> EwStage:
       for j, (b, d) in enumerate(zip(base, dims)):
         if b - origin[j] < 0 or b - origin[j] + sizes[d] > extent[j]:
           raise GenerationError(f'{node} reaches outside {o.name} (dimension {j})')
-    else:  # scalar argument or compile-time values
+    else:  # scalar argument or compile-time values (read at the absolute entry)
       origin = [0] * len(dims)
       strides = [0] * len(dims)
+      for j, (b, d) in enumerate(zip(base, dims)):
+        if b < 0 or b + sizes[d] > o.shape[j]:
+          raise GenerationError(f'{node} reaches outside {o.name} (dimension {j})')
     acc = EwAccess(o, dims, base, origin, strides)
     access[id(node)] = acc
     if store and all(x is not o for x in written):

@@ -73,6 +73,8 @@ EW_LAUNCH_SHAPES = [
   {'strategy': 'generic', 'threads_per_element': 32, 'elements_per_block': 4},
   {'strategy': 'generic', 'threads_per_element': 128, 'elements_per_block': 2},
   {'strategy': 'generic', 'threads_per_element': 8, 'elements_per_block': 16},
+  {'strategy': 'generic', 'threads_per_element': 16, 'elements_per_block': 4, 'points_per_lane': 8},
+  {'strategy': 'generic', 'threads_per_element': 64, 'elements_per_block': 1, 'points_per_lane': 1},
 ]
 
 
@@ -96,7 +98,7 @@ def elementwise_catalogue():
     for fp in ('float', 'double'):
       add(name, fp)
   for v in EW_LAUNCH_SHAPES:
-    for name in ('ew_update', 'ew_feeds_contraction', 'ew_views'):
+    for name in ('ew_update', 'ew_feeds_contraction', 'ew_views', 'ew_control'):
       add(name, 'float', v)
   for v in EW_BENCH_VARIANTS:
     add('ew_update', 'float', v)
@@ -104,8 +106,9 @@ def elementwise_catalogue():
 
 
 EW_BENCH_VARIANTS = [
-  {'strategy': 'generic', 'threads_per_element': g, 'elements_per_block': e}
-  for g, e in ((64, 1), (64, 4), (32, 8), (128, 2), (256, 1), (512, 1))
+  {'strategy': 'generic', 'threads_per_element': g, 'elements_per_block': e, 'points_per_lane': u}
+  for g, e, u in ((64, 1, 1), (64, 1, 4), (64, 1, 8), (64, 4, 4), (32, 8, 4), (128, 2, 4), (256, 1, 2),
+                  (512, 1, 1))
 ]
 
 

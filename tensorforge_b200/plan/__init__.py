@@ -29,8 +29,9 @@ class Plan:
     return f'{self.strategy}:' + ','.join(f'{k}={v}' for k, v in sorted(self.params.items()))
 
 
-def generic_plan(chain, fp_size, threads_per_element=None, elements_per_block=None):
-  """Pick lanes per element and elements per CTA for the generic generator."""
+def generic_plan(chain, fp_size, threads_per_element=None, elements_per_block=None, points_per_lane=None):
+  """Pick lanes per element and elements per CTA for the generic generator (and, for
+  chains with elementwise stages, how many points a lane handles per pass)."""
   from ..codegen.generic import smem_layout
   if threads_per_element is None:
     # measured on B200 over 1,973 random chains (sizes 4..128, 1-4 stages): 64 lanes per
@@ -48,7 +49,10 @@ def generic_plan(chain, fp_size, threads_per_element=None, elements_per_block=No
     raise GenerationError(f'chain needs {total} bytes of shared memory per element group')
   if g * e > 1024:
     e = max(1, 1024 // g)
-  return Plan('generic', {'threads_per_element': g, 'elements_per_block': e}, total, g * e)
+  params = {'threads_per_element': g, 'elements_per_block': e}
+  if chain.has_elementwise():
+    params['points_per_lane'] = points_per_lane or 4
+  return Plan('generic', params, total, g * e)
 
 
 def make_plan(chain, context, variant=None):
@@ -80,4 +84,5 @@ def make_plan(chain, context, variant=None):
           return p
     elif forced in ('colprog', 'tcsplit'):
       raise GenerationError(f'chain does not have the shared-left GEMM form required by {forced}')
-  return generic_plan(chain, fp_size, variant.get('threads_per_element'), variant.get('elements_per_block'))
+  return generic_plan(chain, fp_size, variant.get('threads_per_element'), variant.get('elements_per_block'),
+                      variant.get('points_per_lane'))

@@ -84,8 +84,8 @@ def test_flags_leave_elements_untouched():
   check(results, 'float')
 
 
-@pytest.mark.parametrize('variant', EW_LAUNCH_SHAPES, ids=lambda v: f"G{v['threads_per_element']}E{v['elements_per_block']}")
+@pytest.mark.parametrize('variant', EW_LAUNCH_SHAPES, ids=lambda v: f"G{v['threads_per_element']}E{v['elements_per_block']}U{v.get('points_per_lane', 4)}")
 def test_launch_shapes(variant):
   """Lane groups narrower and wider than a warp, several elements per CTA."""
-  for name in ('ew_update', 'ew_feeds_contraction', 'ew_views'):
+  for name in ('ew_update', 'ew_feeds_contraction', 'ew_views', 'ew_control'):
     check(run_case(name, 77, variant=variant)[0], 'float')
