@@ -10,6 +10,9 @@ generated kernel over all elements. The chain is generated through the public fr
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--variant auto|plain|tf32x3|fp16x3|bf16x3] [--elements E]
+                  [--workload chain_o6|ew_update]
+
+`--workload ew_update` measures the elementwise stage alone instead (its own JSON line).
 
 For N > 1 the driver launches one process per GPU (torchrun); elements are independent, so
 each rank runs its own 500,000 elements (weak scaling) with no collective on the data
@@ -522,6 +525,61 @@ def impl_ours(args, rank, world, dist):
   print(json.dumps(line))
 
 
+def impl_elementwise(args):
+  """`--workload ew_update`: the elementwise stage alone (t = Q*s; O = t > 0 ? t*exp(-t*t) :
+  0.5*t over a 56x9 block per element), default plan, device-resident inputs larger than L2;
+  the oracle timed on a bounded host sample as the CPU figure (the reference cannot emit
+  this path)."""
+  import numpy as np
+  import torch
+  from tensorforge_b200 import workloads as cases
+  from tensorforge_b200.common.basic_types import FloatingPointType
+  from tensorforge_b200.common.context import Context, Options
+  from tensorforge_b200.generators.generator import Generator
+  from tensorforge_b200.runtime import compile_generator
+  torch.cuda.set_device(0)
+  ns = cases.ns_from_module('tensorforge_b200')
+  n = args.elements
+  g = Generator(cases.build_elementwise('ew_update', ns), Context('sm_100a', 'cuda', FloatingPointType.FLOAT, Options()))
+  g.generate()
+  k = compile_generator(g)
+  dev = torch.device('cuda')
+  kw = {'numElements': n}
+  for t, _ in g.abi_symbols():
+    kw[t.name] = 0.5 if t.addressing.name == 'SCALAR' else torch.rand(n * t.get_real_volume(), device=dev) * 2 - 1
+  stream = torch.cuda.current_stream()
+  with Clocks(index=torch.cuda.current_device()) as clocks:
+    total, per = time_launches(lambda: k(**kw), stream, args.steps, max(3, args.warmup))
+  ms = total / args.steps
+  launch = sum(per) / len(per)
+  bytes_el = g.get_chain().bytes_per_element()
+  pk, pk_src = peaks()
+  achieved = n * bytes_el / (launch / 1e3) / 1e9
+  # CPU: the oracle (numpy, FP64) on a bounded sample
+  from oracle import harness, multilinear
+  sample = 2000
+  descrs = cases.build_elementwise('ew_update', ns)
+  lay, mem = harness.make_memory(descrs, sample, seed=1)
+  t0 = time.perf_counter()
+  reps = 0
+  while time.perf_counter() - t0 < 3.0:
+    multilinear.evaluate(descrs, mem, sample)
+    reps += 1
+  cpu_rate = reps * sample / (time.perf_counter() - t0)
+  print(json.dumps({
+    'metric': 'elementwise update throughput', 'value': n / (ms / 1e3), 'unit': 'elements/s', 'n_gpus': 1,
+    'steps': args.steps, 'warmup': max(3, args.warmup), 'ms_per_step': ms, 'higher_is_better': True,
+    'dtype': 'f32', 'data': 'synthetic',
+    'config': {'workload': 'elementwise update, 56x9 block per element, FP32', 'elements': n,
+               'plan': g.get_plan().key(), 'l2': 'inputs larger than L2 (no flush)'},
+    'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': pk['hbm_gbs'], 'unit': 'GB/s',
+                 'frac': achieved / pk['hbm_gbs'], 'traffic': None, 'bytes_per_element': bytes_el,
+                 'peak_source': f'{pk_src} HBM copy bandwidth', 'kernel': g.get_base_name()},
+    'cpu_baseline': {'value': cpu_rate, 'unit': 'elements/s', 'cores': 1, 'kind': 'port',
+                     'sample': f'{sample} elements through the numpy FP64 oracle, repeated for 3 s'},
+    'gpu_launches': args.steps, 'clocks': clocks.summary()}))
+
+
 def main():
   ap = argparse.ArgumentParser()
   ap.add_argument('--gpus', type=int, default=1)
@@ -533,7 +591,12 @@ def main():
   ap.add_argument('--ref-sample', type=int, default=4096)
   ap.add_argument('--no-cpu', action='store_true')
   ap.add_argument('--no-extras', action='store_true')
+  ap.add_argument('--workload', default='chain_o6', choices=['chain_o6', 'ew_update'],
+                  help='chain_o6: the headline order-6 chain; ew_update: the elementwise stage alone')
   args = ap.parse_args()
+  if args.workload == 'ew_update':
+    impl_elementwise(args)
+    return
   from tensorforge_b200.runtime import ranks
   rank, world, _ = ranks.env_rank()
   if args.impl == 'reference':
