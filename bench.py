@@ -368,6 +368,29 @@ def extra_workloads(stream, short=False):
                                'statements': 't = Q*s; O = t > 0 ? t*exp(-t*t) : 0.5*t (56x9, FP32)',
                                'variants': ew}
   bufs.clear()
+  # the order-6 chain with a pointwise update fused as a column-program epilogue, next to
+  # the same chain without it (both plain FP32 column programs)
+  n = 100000 if short else 500000
+  epi = {}
+  for label, descrs in (('chain_only', cases.build(CASE, ns)), ('chain_with_epilogue',
+                                                                cases.build_elementwise('ew_chain_epilogue', ns))):
+    g = Generator(descrs, Context('sm_100a', 'cuda', FloatingPointType.FLOAT, Options()))
+    g.generate()
+    k = compile_generator(g)
+    kw = {'numElements': n}
+    for t, _ in g.abi_symbols():
+      if t.addressing.name == 'SCALAR':
+        kw[t.name] = 0.5
+      else:
+        size = t.spp.count_nz() if t.addressing.name == 'NONE' else n * t.get_real_volume()
+        kw[t.name] = torch.rand(size, device=dev) * 2 - 1
+    total, per = time_launches(lambda: k(**kw), stream, 5, 2)
+    ms = sum(per) / len(per)
+    epi[label] = {'elements_per_s': n / (ms / 1e3), 'ms': ms, 'plan': g.get_plan().key(),
+                  'bytes_per_element': g.get_chain().bytes_per_element()}
+    del kw
+  out['elementwise_epilogue'] = {'elements': n, 'statements': 'out = out > 0 ? out : 0.1*out; out = out + P*s',
+                                 'variants': epi}
   torch.cuda.empty_cache()
   # FP64 order-6 chain
   n = 100000 if short else 500000

@@ -98,6 +98,17 @@ class _ColProg:
   def lit(self, v):
     return self.ctx.fp_type.literal(v)
 
+  def block(self, head):
+    em = self
+
+    class _B:
+      def __enter__(self_):
+        em.open(head)
+
+      def __exit__(self_, *a):
+        em.close()
+    return _B()
+
   def params(self, globals_):
     params = []
     for t, _ in globals_:
@@ -223,6 +234,7 @@ class _ColProg:
       self.w(f'for (int i = 0; i < {s.M}; ++i) {a}[i] = {self.lit(0)};')
     for ti, t in enumerate(s.terms):
       self._term(ti, t)
+    self._epilogue()
     self._store()
 
   def emit(self, globals_):
@@ -465,6 +477,34 @@ class _ColProg:
     self.close()
     self.w('__syncthreads();')
 
+  def _epilogue(self):
+    """Elementwise stages on the finished output column in registers (row i = n0, the
+    thread's column lj = n1), before the store; an accumulated output adds the previous
+    value first, so the statements see the chain's final result."""
+    s = self.s
+    if not s.epilogue:
+      return
+    from .elementwise import RegisterPointEmitter
+    T, M = self.T, s.M
+    counter = [0]
+    for r in range(self.CPT):
+      sf = '' if r == 0 else str(r)
+      self.w(f'// elementwise epilogue ({len(s.epilogue)} stage(s)) on column lj of element el{sf}')
+      self.open(f'if (active{sf})')
+      if s.accumulate:
+        self.w(f'const {T}* const prev = {self._elem_ptr(s.out, "el" + sf)} + (size_t)lj * {M}u;')
+        self.w('#pragma unroll')
+        self.w(f'for (int i = 0; i < {M}; ++i) acc{sf}[i] += prev[i];')
+      for st in s.epilogue:
+        for i in range(M):
+          self.open('')
+          pe = RegisterPointEmitter(self, st, s.out, f'acc{sf}', i, 'lj', M,
+                                    lambda o, sf=sf: self._elem_ptr(o, 'el' + sf), counter)
+          pe.declare_temporaries()
+          pe.statements(st.statements)
+          self.close()
+      self.close()
+
   def _store(self):
     s = self.s
     T, BT, VEC, VT = self.T, self.BT, self.VEC, self.VT
@@ -480,7 +520,7 @@ class _ColProg:
         self.open(f'if (active{sfx(r)})')
         self.w(f'{T}* const col = {self._elem_ptr(o, "el" + sfx(r))} + (size_t)lj * {M}u;')
         self.w('#pragma unroll')
-        op = '+=' if s.accumulate else '='
+        op = '+=' if s.accumulate and not s.epilogue else '='
         self.w(f'for (int i = 0; i < {M}; ++i) col[i] {op} acc{sfx(r)}[i];')
         self.close()
 

@@ -221,6 +221,36 @@ class PointEmitter:
       self.memo = {}
 
 
+class RegisterPointEmitter(PointEmitter):
+  """Point (row, column) of an elementwise epilogue whose output entry is a register.
+
+  The chain's output `out` is read and written as `reg[row]`; other batched operands are
+  read at the same entry of the element through `elem_ptr(op)` (column-major M x N);
+  n0 = row (a constant), n1 = `col` (the thread's column)."""
+
+  def __init__(self, em, stage, out, reg, row, col, M, elem_ptr, counter):
+    super().__init__(em, stage, f'_{row}', counter)
+    self.out, self.reg, self.row, self.col, self.M, self.elem_ptr = out, reg, row, col, M, elem_ptr
+
+  def _index_exprs(self, acc):
+    return [f'({self.row if d == 0 else self.col} + {b})' for d, b in zip(acc.dims, acc.base)]
+
+  def lvalue(self, node):
+    acc = self.stage.access[id(node)]
+    if acc.op is not self.out:
+      raise GenerationError(f'an epilogue writes the chain output only, not {acc.op.name}')
+    return f'{self.reg}[{self.row}]'
+
+  def load(self, node):
+    acc = self.stage.access[id(node)]
+    o = acc.op
+    if o is self.out:
+      return f'{self.reg}[{self.row}]'
+    if o.kind == 'batched':
+      return f'__ldg({self.elem_ptr(o)} + {self.row} + {self.col} * {self.M})'
+    return super().load(node)
+
+
 def multi_point_statements(em, pes, stmts):
   """Statements for several points at once, statement by statement: all points' values
   (their loads in flight together) before any point's store. Points never touch each

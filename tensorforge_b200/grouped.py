@@ -57,8 +57,9 @@ class GroupedKernel:
     for g in generators:
       if g.get_chain() is None:
         g.generate()
-      if match_left_chain(g.get_chain()) is None:
-        raise GenerationError(f'{g.get_base_name()} is not a shared-left chain')
+      shape = match_left_chain(g.get_chain())
+      if shape is None or shape.epilogue:
+        raise GenerationError(f'{g.get_base_name()} is not a shared-left chain without elementwise stages')
       for t, stype in g.abi_symbols():
         if t.addressing == Addressing.SCALAR:
           raise GenerationError('scalar operands are not supported in grouped launches')

@@ -102,6 +102,8 @@ def elementwise_catalogue():
       add(name, 'float', v)
   for v in EW_BENCH_VARIANTS:
     add('ew_update', 'float', v)
+  for name in ('ew_chain_epilogue', 'ew_chain_epilogue_add'):
+    add(name, 'float', {'strategy': 'generic'})
   return out
 
 

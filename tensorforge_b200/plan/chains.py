@@ -15,7 +15,7 @@ or a single `out (+)= A x B`. All operands must span their full shape (bounding 
 shape) so that columns are contiguous. This is the shape of BASELINE configs 0-3
 (benchmarks/fused/programs/s3time.cf) and of SeisSol's volume/local kernels.
 """
-from dataclasses import dataclass
+from dataclasses import dataclass, field
 from typing import List, Optional
 
 from ..common.basic_types import DataFlowDirection
@@ -38,6 +38,7 @@ class LeftChain:
   M: int
   N: int
   accumulate: bool   # out_e += ... (previous value read once)
+  epilogue: list = field(default_factory=list)   # elementwise stages on the output, per entry
 
 
 def _full(op):
@@ -50,9 +51,36 @@ def _full_ref(stage, ref):
   return [l for l, _ in box] == [0] * len(box) and [u for _, u in box] == list(ref.op.shape)
 
 
+def _is_elementwise(stage):
+  return getattr(stage, 'kind', '') == 'elementwise'
+
+
+def _epilogue_ok(tail, shape):
+  """Elementwise stages that can run on the output's registers: over the output's whole
+  M x N box, writing the output only, reading the output, scalars and batched dense M x N
+  tensors at the same entry (n0 = row, n1 = column)."""
+  out = shape.out
+  for s in tail:
+    if s.sizes != [shape.M, shape.N] or any(o is not out for o in s.written):
+      return False
+    for acc in s.access.values():
+      o = acc.op
+      if o.kind in ('scalar', 'data') and not acc.dims:
+        continue
+      if o.kind != 'batched' or o.sparse or not _full(o) or list(o.shape) != [shape.M, shape.N]:
+        return False
+      if acc.dims != [0, 1] or acc.base != [0, 0]:
+        return False
+  return True
+
+
 def match_left_chain(chain) -> Optional[LeftChain]:
+  """The chain's shared-left form, with trailing elementwise stages as an epilogue."""
   st = chain.stages
-  if not st:
+  k = next((i for i, s in enumerate(st) if _is_elementwise(s)), len(st))
+  tail = st[k:]
+  st = st[:k]
+  if not st or not all(_is_elementwise(s) for s in tail):
     return None
   for s in st:
     if not s.is_matmul():
@@ -115,7 +143,12 @@ def match_left_chain(chain) -> Optional[LeftChain]:
       return None
     if t.B is out or t.A is out or t.R is out:
       return None
-  return LeftChain(terms, out, M, N, accumulate)
+  shape = LeftChain(terms, out, M, N, accumulate)
+  if tail:
+    if not _epilogue_ok(tail, shape):
+      return None
+    shape.epilogue = list(tail)
+  return shape
 
 
 def a_values(term):
@@ -198,10 +231,14 @@ def colprog_plan(chain, shape: LeftChain, fp_size, variant):
 
 
 def tcsplit_plan(chain, shape, precision, variant):
+  if shape.epilogue:  # elementwise epilogues run on the column programs only
+    return None
   from ..codegen import tcsplit
   return tcsplit.plan(chain, shape, precision, variant)
 
 
 def dmma_plan(chain, shape, variant):
+  if shape.epilogue:
+    return None
   from ..codegen import dmma
   return dmma.plan(chain, shape, variant, SMEM_LIMIT)

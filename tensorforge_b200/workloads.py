@@ -366,6 +366,25 @@ def ew_sparse_read(ns, rows=14, cols=9, seed=4):
   return [ns.ElementwiseDescr([ot.assign(ot.tensor(O), 2.0 * ot.tensor(S) + 1.0)])]
 
 
+def ew_chain_epilogue(ns, basis=56, quantities=9, terms=3, seed=0, accumulate=False):
+  """The volume chain followed by a pointwise update of its output, fused as an epilogue of
+  the column program:  out = sum_t K_t Q S_t (+ out);  out = out > 0 ? out : 0.1 * out;
+  out = out + P * s  (P a second per-element 56x9 input, s a scalar)."""
+  ot = ns.optree
+  descrs = volume_chain(ns, basis=basis, quantities=quantities, terms=terms, seed=seed)
+  out = descrs[-1].dest.tensor
+  if accumulate:
+    descrs[1].add = True
+  P = ns.Tensor([basis, quantities], ns.Addressing.STRIDED)
+  s = ns.Tensor([], ns.Addressing.SCALAR)
+  o = ot.tensor(out)
+  descrs.append(ns.ElementwiseDescr([
+    ot.assign(o, ot.ternary(o > 0.0, o, 0.1 * o)),
+    ot.assign(o, o + ot.tensor(P) * ot.scalar(s)),
+  ]))
+  return descrs
+
+
 EW_CASES = {
   # name: (builder, kwargs, num_elements)
   'ew_update': (ew_update, {}, 37),
@@ -375,6 +394,8 @@ EW_CASES = {
   'ew_feeds_contraction': (ew_feeds_contraction, {}, 11),
   'ew_views': (ew_views, {}, 7),
   'ew_sparse_read': (ew_sparse_read, {}, 13),
+  'ew_chain_epilogue': (ew_chain_epilogue, {}, 29),
+  'ew_chain_epilogue_add': (ew_chain_epilogue, {'basis': 20, 'quantities': 9, 'accumulate': True, 'seed': 2}, 23),
 }
 
 

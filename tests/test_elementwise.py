@@ -335,3 +335,50 @@ def test_yateto_add_scalar():
   assert [t.alias for t, _ in g.abi_symbols()] == ['Q', 'dt', 'O']
   assert [c for c, _ in g.abi_params()][:5] == ['const float**', 'unsigned', 'float', 'float**', 'unsigned']
   assert 'const_cast<const float**>(Q)' in cpp[0] and 'extraOffset_O' in cpp[0]
+
+
+# ------------------------------------------------------------------ epilogues on the column program
+@pytest.mark.parametrize('name', ['ew_chain_epilogue', 'ew_chain_epilogue_add'])
+def test_oracle_chain_epilogue_by_hand(name):
+  fn, kw, n = W.EW_CASES[name]
+  full = fn(NS, **kw)
+  chain = W.volume_chain(NS, basis=kw.get('basis', 56), quantities=kw.get('quantities', 9), seed=kw.get('seed', 0))
+  if kw.get('accumulate'):
+    chain[1].add = True
+  lay_f, mem_f = harness.make_memory(full, n, seed=5)
+  lay_c, mem_c = harness.make_memory(chain, n, seed=5)
+  for name_ in mem_c.buffers:  # the chain's operands are drawn first, identically
+    assert np.array_equal(mem_c.buffers[name_], mem_f.buffers[name_])
+  before = {k: v.copy() for k, v in mem_f.buffers.items()}
+  multilinear.evaluate(full, mem_f, n)
+  multilinear.evaluate(chain, mem_c, n)
+  lay = {l.name: l for l in lay_f}
+  out = [l.name for l in lay_c if l.tensor is chain[1].dest.tensor][0]
+  s = mem_f.scalars['m9']
+  for e in range(n):
+    c = _block(lay[out], mem_c.buffers[out], e)
+    want = np.where(c > 0, c, 0.1 * c) + _block(lay['m8'], before['m8'], e) * s
+    assert np.allclose(_block(lay[out], mem_f.buffers[out], e), want, rtol=1e-13, atol=1e-13)
+
+
+def test_epilogue_plans():
+  for fp in (FP.FLOAT, FP.DOUBLE):
+    g = _gen(W.build_elementwise('ew_chain_epilogue', NS), fp)
+    assert g.get_plan().strategy == 'colprog', g.get_plan()
+    assert '// elementwise epilogue' in g.get_kernel()
+  # tensor-core precision requested: the epilogue keeps the chain on the column program
+  g = Generator(W.build_elementwise('ew_chain_epilogue', NS),
+                Context('sm_100a', 'cuda', FP.FLOAT, Options(precision='tf32x3')))
+  g.generate()
+  assert g.get_plan().strategy == 'colprog'
+  # an elementwise stage that writes another tensor is not an epilogue: generic generator
+  d = W.volume_chain(NS, basis=20, quantities=9)
+  out = d[-1].dest.tensor
+  other = Tensor([20, 9], Addressing.STRIDED)
+  d.append(ElementwiseDescr([ot.assign(ot.tensor(other), ot.tensor(out) * 2.0)]))
+  assert _gen(d).get_plan().strategy == 'generic'
+  # one between the contractions: generic as well
+  d = W.volume_chain(NS, basis=20, quantities=9, terms=2)
+  out = d[-1].dest.tensor
+  d.insert(2, ElementwiseDescr([ot.assign(ot.tensor(out), ot.tensor(out) * 2.0)]))
+  assert _gen(d).get_plan().strategy == 'generic'

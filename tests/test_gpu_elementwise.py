@@ -89,3 +89,20 @@ def test_launch_shapes(variant):
   """Lane groups narrower and wider than a warp, several elements per CTA."""
   for name in ('ew_update', 'ew_feeds_contraction', 'ew_views', 'ew_control'):
     check(run_case(name, 77, variant=variant)[0], 'float')
+
+
+@pytest.mark.parametrize('name', ['ew_chain_epilogue', 'ew_chain_epilogue_add'])
+def test_epilogue_column_program_and_generic_agree_with_oracle(name):
+  """The fused epilogue (column program) and the same descriptors on the generic generator."""
+  res, g = run_case(name, 333)
+  assert g.get_plan().strategy == 'colprog'
+  check(res, 'float')
+  res, g = run_case(name, 333, variant={'strategy': 'generic'})
+  assert g.get_plan().strategy == 'generic'
+  check(res, 'float')
+
+
+def test_epilogue_flags():
+  n = 250
+  flags = (np.arange(n) % 4 != 2).astype(np.int32)
+  check(run_case('ew_chain_epilogue', n, flags=flags)[0], 'float')
