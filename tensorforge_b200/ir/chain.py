@@ -215,10 +215,8 @@ class Chain:
       vol = o.storage_size() if o.sparse else _touched_volume(self, o)
       if d == DataFlowDirection.SOURCE:
         total += vol * size
-      elif d == DataFlowDirection.SINK:
+      else:  # written (and possibly read back): read from memory only before the first overwrite
         total += vol * size * (2 if _reads_dest(self, o) else 1)
-      else:
-        total += 2 * vol * size
       if o.addressing == Addressing.PTR_BASED:
         total += 8
     return total
@@ -230,15 +228,15 @@ def _touched_volume(chain, o):
 
 
 def _reads_dest(chain, o):
-  first = True
+  """True when the chain reads o's previous contents from memory: a read, or an
+  accumulating write, before the first plain overwrite (later reads see the chain's own
+  result, not HBM data the algorithm has to move)."""
   for s in chain.stages:
     if any(r.op is o for r in s.ops):
       return True
     written = any(x is o for x in s.written) if getattr(s, 'kind', '') == 'elementwise' else (s.dest is o)
     if written:
-      if s.add and first:
-        return True
-      first = False
+      return bool(s.add)
   return False
 
 
