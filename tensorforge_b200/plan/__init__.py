@@ -34,9 +34,10 @@ def generic_plan(chain, fp_size, threads_per_element=None, elements_per_block=No
   chains with elementwise stages, how many points a lane handles per pass)."""
   from ..codegen.generic import smem_layout
   if threads_per_element is None:
-    # measured on B200 over 1,973 random chains (sizes 4..128, 1-4 stages): 64 lanes per
-    # element with one element per CTA is the fastest generic variant for most chains
-    threads_per_element = 64
+    # measured on B200 over 1,973 random chains (sizes 4..128, 1-4 stages, lane groups of
+    # 4..256): 256 lanes per element with one element per CTA is the fastest generic
+    # variant for most chains (1,140 of them; the next, 256 x 2, for 237)
+    threads_per_element = 256
   g = threads_per_element
   e = elements_per_block if elements_per_block is not None else 1
   while True:
