@@ -149,6 +149,19 @@ def smem_plan_v2(shape, precision):
 def plan(chain, shape, precision, variant):
   if precision not in KSTEP:
     return None
+  # operand form B (codegen/tcsplit_b.py) is opt-in (variant {'form': 'b'}): it is the more
+  # accurate form (the per-element input is split directly, rel. L2 1.5e-7 against 3.9e-7 on
+  # the order-6 chain) but measured slower than form U below (2.7e8 against 4.8e8 el/s)
+  form = variant.get('form', 'u')
+  if precision == 'tf32x3' and form == 'b':
+    # operand form B (codegen/tcsplit_b.py) when every term reads the same per-element input
+    from .tcsplit_b import layout_b
+    lb = layout_b(shape)
+    if lb is not None:
+      return Plan('tcsplit', {'precision': precision, 'form': 'b'}, max(lb['total'], 120 * 1024), 32 * (4 * H_GROUPS + 1),
+                  note=f'form B: M={shape.M} N={shape.N} terms={len(shape.terms)} tile={lb["te"]} smem={lb["total"]}')
+    if variant.get('form') == 'b':
+      return None
   if shape.M > 256 or shape.N > 128:
     return None
   lay = layout(shape, precision)
@@ -292,6 +305,9 @@ __device__ __forceinline__ void bulk_wait() { asm volatile("cp.async.bulk.wait_g
 
 def emit_tcsplit(chain, plan_, context, base_name, globals_):
   shape = match_left_chain(chain)
+  if plan_.params.get('form') == 'b':
+    from .tcsplit_b import _TCB
+    return _TCB(chain, shape, plan_, context, base_name).emit(globals_)
   return _TC(chain, shape, plan_, context, base_name).emit(globals_)
 
 

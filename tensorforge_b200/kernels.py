@@ -18,6 +18,10 @@ EXTRA = [
   ('chain_o6', 'float', {'precision': 'bf16x3'}),
   ('chain_o4_q27', 'float', {'precision': 'tf32x3'}),
   ('chain_o6', 'float', {'precision': 'tf32x3', 'variant': {'pipe': 1}}),
+  ('chain_o6', 'float', {'precision': 'tf32x3', 'variant': {'form': 'u'}}),
+  ('chain_o6', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b'}}),
+  ('c0_gemm_ptr', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b'}}),
+  ('c0_gemm_strided', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b'}}),
   ('c0_gemm_ptr', 'float', {'precision': 'tf32x3'}),
   ('c0_gemm_strided', 'float', {'precision': 'tf32x3'}),
   ('gemm_add', 'float', {'precision': 'tf32x3'}),

@@ -125,3 +125,39 @@ def test_other_chains_on_tensor_cores(case):
   got, ref, _, _ = _run(case, 'tf32x3', 203)
   rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
   assert rel <= 1e-6, rel
+
+
+FORM_U = {'form': 'u'}
+FORM_B = {'form': 'b'}
+
+
+@pytest.mark.parametrize('form', [FORM_B, FORM_U], ids=['formB', 'formU'])
+@pytest.mark.parametrize('n', [1, 7, 8, 333, 4099])
+def test_chain_o6_both_operand_forms(form, n):
+  """Operand form B (the per-element input as the MMA B operand, R applied in the epilogue)
+  and form U (U = B R formed on CUDA cores, the MMA A operand in tensor memory)."""
+  got, ref, _, _ = _run('chain_o6', 'tf32x3', n, variant=dict(form))
+  rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+  assert rel <= 1e-6, rel
+
+
+@pytest.mark.parametrize('case', ['c0_gemm_ptr', 'c0_gemm_strided'])
+def test_form_b_single_term(case):
+  """One term (the A block stacked with itself, elements split between the lane halves),
+  pointer-array and strided operands, no R."""
+  from tensorforge_b200.kernels import make
+  assert make(case, 'float', precision='tf32x3', variant=dict(FORM_B)).get_plan().params.get('form') == 'b'
+  got, ref, _, _ = _run(case, 'tf32x3', 1001, variant=dict(FORM_B))
+  rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+  assert rel <= 1e-6, rel
+
+
+def test_form_b_flags_and_loguniform():
+  got, ref, out, flags = _run('chain_o6', 'tf32x3', 611, use_flags=True, variant=dict(FORM_B))
+  rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+  assert rel <= 1e-6, rel
+  for e in np.nonzero(flags == 0)[0][:5]:
+    s = out.starts[e]
+    assert np.array_equal(got[s:s + 504], ref[s:s + 504])
+  got, ref, _, _ = _run('chain_o6', 'tf32x3', 777, dist='loguniform', variant=dict(FORM_B))
+  assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-6
