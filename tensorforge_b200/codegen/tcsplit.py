@@ -149,16 +149,18 @@ def smem_plan_v2(shape, precision):
 def plan(chain, shape, precision, variant):
   if precision not in KSTEP:
     return None
-  # operand form B (codegen/tcsplit_b.py) is opt-in (variant {'form': 'b'}): it is the more
-  # accurate form (the per-element input is split directly, rel. L2 1.5e-7 against 3.9e-7 on
-  # the order-6 chain) but measured slower than form U below (2.7e8 against 4.8e8 el/s)
+  # operand form B (codegen/tcsplit_b.py) is opt-in (variant {'form': 'b'}): measured on the
+  # order-6 chain at 3.0e8 (13-element tiles, one B buffer) and 3.7e8 el/s (8-element tiles,
+  # two B buffers) against 4.8e8 for form U below
   form = variant.get('form', 'u')
   if precision == 'tf32x3' and form == 'b':
     # operand form B (codegen/tcsplit_b.py) when every term reads the same per-element input
     from .tcsplit_b import layout_b
-    lb = layout_b(shape)
+    acc, bbuf = int(variant.get('acc', 1)), int(variant.get('bbuf', 1))
+    lb = layout_b(shape, acc, bbuf, variant.get('te'))
     if lb is not None:
-      return Plan('tcsplit', {'precision': precision, 'form': 'b'}, max(lb['total'], 120 * 1024), 32 * (4 * H_GROUPS + 1),
+      params = {'precision': precision, 'form': 'b', 'acc': acc, 'bbuf': bbuf, 'te': lb['te']}
+      return Plan('tcsplit', params, max(lb['total'], 120 * 1024), 32 * (4 * H_GROUPS + 1),
                   note=f'form B: M={shape.M} N={shape.N} terms={len(shape.terms)} tile={lb["te"]} smem={lb["total"]}')
     if variant.get('form') == 'b':
       return None

@@ -55,7 +55,7 @@ __device__ __forceinline__ void ld_x4(unsigned taddr, unsigned* v) {
 '''
 
 MAX_ROWS = 64      # rows of one stacked term (half of the 128 lanes)
-MAX_N = 64         # flat columns per tile (TMEM: 2 buffers x 2 blocks x 2 accumulators x 64)
+SMEM_MAX = 227 * 1024
 
 
 def blocks_of(nterms):
@@ -72,8 +72,50 @@ def blocks_of(nterms):
   return None
 
 
-def layout_b(shape):
-  """Sizes and shared-memory offsets of form B, or None when the chain does not fit it."""
+def _sizes(shape, te, acc, bbuf):
+  terms = shape.terms
+  B = terms[0].B
+  K, P, M, N = terms[0].K, terms[0].P, shape.M, shape.N
+  n_mma = _pad(te * P, 16)
+  kpad = _pad(K, 8)
+  blocks = blocks_of(len(terms))
+  a_bytes = 128 * kpad * 4
+  b_bytes = n_mma * kpad * 4
+  vol_b = _pad(B.element_volume(), 4)
+  r_off, r_vals = {}, 0
+  for ti, t in enumerate(terms):
+    if t.R is not None:
+      r_off[ti] = r_vals
+      r_vals += te * _pad(t.R.storage_size(), 4)
+  vol_o = M * N
+  off = 0
+  off_a = off
+  off += len(blocks) * 2 * a_bytes
+  off_b = off
+  off += bbuf * 2 * b_bytes
+  off_raw = off
+  off += _pad(te * vol_b * 4, 128)
+  off_r = off
+  off += _pad(2 * r_vals * 4, 128)
+  off_out = off
+  off += _pad(te * vol_o * 4, 128)
+  off_bar = off
+  total = off + 256
+  tmem = 2 * len(blocks) * acc * n_mma
+  return dict(te=te, n_mma=n_mma, kpad=kpad, K=K, P=P, M=M, N=N, blocks=blocks, a_bytes=a_bytes,
+              b_bytes=b_bytes, vol_b=vol_b, r_off=r_off, r_vals=r_vals, vol_o=vol_o, off_a=off_a, off_b=off_b,
+              off_raw=off_raw, off_r=off_r, off_out=off_out, off_bar=off_bar, total=total,
+              hsplit=(te + 1) // 2, acc=acc, bbuf=bbuf, tmem=tmem)
+
+
+def layout_b(shape, acc=1, bbuf=1, te=None):
+  """Sizes and shared-memory offsets of form B, or None when the chain does not fit it.
+
+  acc: accumulators per block (1: all three split products in one; 2: hi*hi apart from the
+  cross terms); bbuf: B tiles in shared memory (2 lets the producers split tile n+1 while the
+  tensor cores still read tile n). The tile is the largest number of whole elements whose
+  flat columns (padded to 16, at most 256) fit two accumulator sets in the 512 TMEM columns
+  and whose buffers fit in shared memory."""
   terms = shape.terms
   if len(terms) < 1 or len(terms) > 4 or shape.accumulate or shape.epilogue:
     return None
@@ -94,40 +136,14 @@ def layout_b(shape):
   out = shape.out
   if out.addressing.name not in ('STRIDED', 'PTR_BASED') or out.sparse:
     return None
-  te = MAX_N // P
-  if te < 1:
-    return None
-  n_mma = _pad(te * P, 16)
-  kpad = _pad(K, 8)
-  blocks = blocks_of(len(terms))
-  a_bytes = 128 * kpad * 4
-  b_bytes = n_mma * kpad * 4
-  vol_b = _pad(B.element_volume(), 4)
-  r_terms = [ti for ti, t in enumerate(terms) if t.R is not None]
-  r_off, r_vals = {}, 0
-  for ti in r_terms:
-    r_off[ti] = r_vals
-    r_vals += te * _pad(terms[ti].R.storage_size(), 4)
-  vol_o = M * N
-  off = 0
-  off_a = off
-  off += len(blocks) * 2 * a_bytes
-  off_b = off
-  off += 2 * 2 * b_bytes
-  off_raw = off
-  off += _pad(te * vol_b * 4, 128)
-  off_r = off
-  off += _pad(2 * r_vals * 4, 128)
-  off_out = off
-  off += _pad(te * vol_o * 4, 128)
-  off_bar = off
-  total = off + 256
-  if total > 227 * 1024:
-    return None
-  return dict(te=te, n_mma=n_mma, kpad=kpad, K=K, P=P, M=M, N=N, blocks=blocks, a_bytes=a_bytes,
-              b_bytes=b_bytes, vol_b=vol_b, r_off=r_off, r_vals=r_vals, vol_o=vol_o, off_a=off_a, off_b=off_b,
-              off_raw=off_raw, off_r=off_r, off_out=off_out, off_bar=off_bar, total=total,
-              hsplit=(te + 1) // 2)
+  cands = [te] if te is not None else range(256 // P, 0, -1)
+  for t_e in cands:
+    if t_e < 1 or _pad(t_e * P, 16) > 256:
+      continue
+    L = _sizes(shape, t_e, acc, bbuf)
+    if L['tmem'] <= 512 and L['total'] <= SMEM_MAX:
+      return L
+  return None
 
 
 class _TCB:
@@ -139,7 +155,8 @@ class _TCB:
     self.plan = plan_
     self.ctx = ctx
     self.base = base
-    self.L = layout_b(shape)
+    p = plan_.params
+    self.L = layout_b(shape, p.get('acc', 1), p.get('bbuf', 1), p.get('te'))
     self.lines = []
     self.ind = 0
 
@@ -214,8 +231,8 @@ class _TCB:
 
   def _col(self, buf, blk, acc):
     L = self.L
-    nb = len(L['blocks'])
-    return f'({buf}) * {nb * 2 * L["n_mma"]}u + {blk * 2 * L["n_mma"] + acc * L["n_mma"]}u'
+    nb, na = len(L['blocks']), L['acc']
+    return f'({buf}) * {nb * na * L["n_mma"]}u + {(blk * na + acc) * L["n_mma"]}u'
 
   def emit(self, globals_):
     s, L, b = self.s, self.L, self.base
@@ -323,29 +340,34 @@ class _TCB:
     self.open('if (lane == 0)')
     self.w('unsigned it = 0;')
     self.open('for (size_t tile = blockIdx.x; tile < numTiles && ok; tile += gridDim.x, ++it)')
-    self.w('const unsigned sb = it & 1u;')
-    self.w(f'if (!tfb_tc::mbar_wait(&bars[{BAR_BFULL} + sb], (it >> 1) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 50u); break; }}')
+    bsel, bfull_par, _, _ = self._bbuf_exprs()
+    self.w('const unsigned sb = it & 1u;             // accumulator set')
+    self.w(f'const unsigned bs = {bsel};             // B tile buffer')
+    self.w(f'if (!tfb_tc::mbar_wait(&bars[{BAR_BFULL} + bs], {bfull_par}, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 50u); break; }}')
     self.w(f'if (it >= 2u && !tfb_tc::mbar_wait(&bars[{BAR_DFREE} + sb], ((it - 2u) >> 1) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 51u); break; }}')
     self.w('tfb_tc::fence_after();')
-    self.w(f'const unsigned bhi = tfb_tc::smem_u32(tfb_smem_raw + {L["off_b"]}) + sb * {2 * L["b_bytes"]}u;')
+    self.w(f'const unsigned bhi = tfb_tc::smem_u32(tfb_smem_raw + {L["off_b"]}) + bs * {2 * L["b_bytes"]}u;')
     self.w(f'const unsigned blo = bhi + {L["b_bytes"]}u;')
     for blk in range(nb):
       hi_off = L['off_a'] + blk * 2 * L['a_bytes']
       self.open('')
       self.w(f'const unsigned ahi = tfb_tc::smem_u32(tfb_smem_raw + {hi_off});')
       self.w(f'const unsigned alo = ahi + {L["a_bytes"]}u;')
-      self.w(f'const unsigned dm = tmem + {self._col("sb", blk, 0)}, dc = tmem + {self._col("sb", blk, 1)};')
+      if L['acc'] == 2:
+        self.w(f'const unsigned dm = tmem + {self._col("sb", blk, 0)}, dc = tmem + {self._col("sb", blk, 1)};')
+      else:  # one accumulator takes all three split products
+        self.w(f'const unsigned dm = tmem + {self._col("sb", blk, 0)}, dc = dm;')
       self.open(f'for (int ks = 0; ks < {ksteps}; ++ks)')
       self.w(f'const uint64_t ah = tfb_tc::smem_desc(ahi + ks * 256u, 128u, {sbo_a}u);')
       self.w(f'const uint64_t al = tfb_tc::smem_desc(alo + ks * 256u, 128u, {sbo_a}u);')
       self.w(f'const uint64_t bh = tfb_tc::smem_desc(bhi + ks * 256u, 128u, {sbo_b}u);')
       self.w(f'const uint64_t bl = tfb_tc::smem_desc(blo + ks * 256u, 128u, {sbo_b}u);')
       self.w(f'tfb_tcb::mma_ss_tf32(dm, ah, bh, {idesc}u, ks > 0 ? 1u : 0u);')
-      self.w(f'tfb_tcb::mma_ss_tf32(dc, ah, bl, {idesc}u, ks > 0 ? 1u : 0u);')
+      self.w(f'tfb_tcb::mma_ss_tf32(dc, ah, bl, {idesc}u, {"ks > 0 ? 1u : 0u" if L["acc"] == 2 else "1u"});')
       self.w(f'tfb_tcb::mma_ss_tf32(dc, al, bh, {idesc}u, 1u);')
       self.close()
       self.close()
-    self.w(f'tfb_tc::mma_commit(&bars[{BAR_BFREE} + sb]);')
+    self.w(f'tfb_tc::mma_commit(&bars[{BAR_BFREE} + bs]);')
     self.w(f'tfb_tc::mma_commit(&bars[{BAR_DFULL} + sb]);')
     self.close()
     self.close()
@@ -404,10 +426,11 @@ class _TCB:
     self.open('if (more)')
     self.w(f'if (!tfb_tc::mbar_wait(&bars[{BAR_STAGE}], it & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 60u); }}')
     self.w('pending = false;')
-    self.w(f'if (it >= 2u && !tfb_tc::mbar_wait(&bars[{BAR_BFREE} + (it & 1u)], ((it - 2u) >> 1) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 61u); }}')
-    self._split(NP)
+    bsel, _, free_cond, free_par = self._bbuf_exprs()
+    self.w(f'if ({free_cond} && !tfb_tc::mbar_wait(&bars[{BAR_BFREE} + {bsel}], {free_par}, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 61u); }}')
+    self._split(NP, bsel)
     self.w('tfb_tc::fence_proxy_async();')
-    self.w(f'tfb_tc::mbar_arrive(&bars[{BAR_BFULL} + (it & 1u)]);')
+    self.w(f'tfb_tc::mbar_arrive(&bars[{BAR_BFULL} + {bsel}]);')
     self.close()
     self.w(f'tfb_tc::named_sync(1, {NP});   // the raw stage has been read')
     self.open('if (has_next)')
@@ -430,24 +453,35 @@ class _TCB:
     self.w('if (ptid == 0) tfb_tc::bulk_wait();')
     self.close()
 
-  def _split(self, NP):
+  def _bbuf_exprs(self):
+    """(buffer of tile `it`, BFULL parity, BFREE wait condition, BFREE parity)."""
+    if self.L['bbuf'] == 1:
+      return '0u', 'it & 1u', 'it >= 1u', '(it - 1u) & 1u'
+    return '(it & 1u)', '(it >> 1) & 1u', 'it >= 2u', '((it - 2u) >> 1) & 1u'
+
+  def _split(self, NP, bsel):
     """raw stage (column-major K x P per element) -> B tile hi / lo in canonical K-major layout;
-    row n = flat column (e, m), K contiguous (a column of B_e), 4 values per item."""
+    row n = flat column (e, m), K contiguous (a column of B_e), 4 values per item. Consecutive
+    threads take consecutive rows n, so each 8-row core matrix is one conflict-free 128-byte
+    store; lo = value - hi is passed unrounded (the tensor core reads its TF32 part)."""
     L = self.L
     te, kpad, K, P = L['te'], L['kpad'], L['K'], L['P']
     k4 = kpad // 4
+    nr = te * P
     sbo = (kpad // 4) * 128
     self.open('')
-    self.w(f'unsigned char* const bh = tfb_smem_raw + {L["off_b"]} + (it & 1u) * {2 * L["b_bytes"]}u;')
+    self.w(f'unsigned char* const bh = tfb_smem_raw + {L["off_b"]} + {bsel} * {2 * L["b_bytes"]}u;')
     self.w(f'unsigned char* const bl = bh + {L["b_bytes"]}u;')
-    self.open(f'for (unsigned q = ptid; q < {te * P * k4}u; q += {NP}u)')
-    self.w(f'const unsigned n = q / {k4}u, l4 = q - n * {k4}u;')
+    self.open(f'for (unsigned q = ptid; q < {nr * k4}u; q += {NP}u)')
+    self.w(f'const unsigned l4 = q / {nr}u, n = q - l4 * {nr}u;')
     self.w(f'const unsigned ei = n / {P}u, m = n - ei * {P}u;')
     self.w('float4 x = make_float4(0.0f, 0.0f, 0.0f, 0.0f);')
     self.w(f'if (l4 < {K // 4}u) x = *reinterpret_cast<const float4*>(raw + ei * {L["vol_b"]}u + m * {K}u + 4u * l4);')
     self.w('uint4 h, l;')
-    self.w('tfb_tc::tf32_split(x.x, h.x, l.x); tfb_tc::tf32_split(x.y, h.y, l.y);')
-    self.w('tfb_tc::tf32_split(x.z, h.z, l.z); tfb_tc::tf32_split(x.w, h.w, l.w);')
+    self.w('h.x = tfb_tc::tf32_rna(x.x); l.x = __float_as_uint(x.x - __uint_as_float(h.x));')
+    self.w('h.y = tfb_tc::tf32_rna(x.y); l.y = __float_as_uint(x.y - __uint_as_float(h.y));')
+    self.w('h.z = tfb_tc::tf32_rna(x.z); l.z = __float_as_uint(x.z - __uint_as_float(h.z));')
+    self.w('h.w = tfb_tc::tf32_rna(x.w); l.w = __float_as_uint(x.w - __uint_as_float(h.w));')
     self.w(f'const unsigned off = (n >> 3) * {sbo}u + l4 * 128u + (n & 7u) * 16u;')
     self.w('*reinterpret_cast<uint4*>(bh + off) = h;')
     self.w('*reinterpret_cast<uint4*>(bl + off) = l;')
@@ -476,11 +510,17 @@ class _TCB:
     t = s.terms[ti]
     nmma = L['n_mma']
     self.open('')
-    self._ld_cols(f'(lane_addr + pb * {len(L["blocks"]) * 2 * nmma}u)', blk * 2 * nmma + e * P, 'wm', P)
-    self._ld_cols(f'(lane_addr + pb * {len(L["blocks"]) * 2 * nmma}u)', blk * 2 * nmma + nmma + e * P, 'wc', P)
+    na = L['acc']
+    base = f'(lane_addr + pb * {len(L["blocks"]) * na * nmma}u)'
+    self._ld_cols(base, blk * na * nmma + e * P, 'wm', P)
+    if na == 2:
+      self._ld_cols(base, blk * na * nmma + nmma + e * P, 'wc', P)
     self.w('tfb_tc::ld_wait();')
     for m in range(P):
-      self.w(f'const float w{m} = __uint_as_float(wm[{m}]) + __uint_as_float(wc[{m}]);')
+      if na == 2:
+        self.w(f'const float w{m} = __uint_as_float(wm[{m}]) + __uint_as_float(wc[{m}]);')
+      else:
+        self.w(f'const float w{m} = __uint_as_float(wm[{m}]);')
     if t.R is None:
       for j in range(N):
         self.w(f'{acc_name}[{j}] += w{j};')

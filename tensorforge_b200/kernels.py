@@ -22,6 +22,10 @@ EXTRA = [
   ('chain_o6', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b'}}),
   ('c0_gemm_ptr', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b'}}),
   ('c0_gemm_strided', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b'}}),
+  ('chain_o6', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b', 'acc': 2, 'bbuf': 2}}),
+  ('chain_o6', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b', 'bbuf': 2}}),
+  ('c0_gemm_ptr', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b', 'acc': 2, 'bbuf': 2}}),
+  ('c0_gemm_strided', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b', 'acc': 2, 'bbuf': 2}}),
   ('c0_gemm_ptr', 'float', {'precision': 'tf32x3'}),
   ('c0_gemm_strided', 'float', {'precision': 'tf32x3'}),
   ('gemm_add', 'float', {'precision': 'tf32x3'}),

@@ -131,7 +131,10 @@ FORM_U = {'form': 'u'}
 FORM_B = {'form': 'b'}
 
 
-@pytest.mark.parametrize('form', [FORM_B, FORM_U], ids=['formB', 'formU'])
+FORM_B_2ACC = {'form': 'b', 'acc': 2, 'bbuf': 2}
+
+
+@pytest.mark.parametrize('form', [FORM_B, FORM_B_2ACC, FORM_U], ids=['formB', 'formB_2acc_2buf', 'formU'])
 @pytest.mark.parametrize('n', [1, 7, 8, 333, 4099])
 def test_chain_o6_both_operand_forms(form, n):
   """Operand form B (the per-element input as the MMA B operand, R applied in the epilogue)
@@ -141,13 +144,14 @@ def test_chain_o6_both_operand_forms(form, n):
   assert rel <= 1e-6, rel
 
 
+@pytest.mark.parametrize('form', [FORM_B, FORM_B_2ACC], ids=['formB', 'formB_2acc_2buf'])
 @pytest.mark.parametrize('case', ['c0_gemm_ptr', 'c0_gemm_strided'])
-def test_form_b_single_term(case):
+def test_form_b_single_term(case, form):
   """One term (the A block stacked with itself, elements split between the lane halves),
   pointer-array and strided operands, no R."""
   from tensorforge_b200.kernels import make
-  assert make(case, 'float', precision='tf32x3', variant=dict(FORM_B)).get_plan().params.get('form') == 'b'
-  got, ref, _, _ = _run(case, 'tf32x3', 1001, variant=dict(FORM_B))
+  assert make(case, 'float', precision='tf32x3', variant=dict(form)).get_plan().params.get('form') == 'b'
+  got, ref, _, _ = _run(case, 'tf32x3', 1001, variant=dict(form))
   rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
   assert rel <= 1e-6, rel
 
