@@ -13,18 +13,20 @@ this form computes W_t = A_t * B_e on the tensor cores and applies R_{e,t} in th
     once per CTA into hi + lo, B_e split per tile by the producers straight from the staged
     column-major input (a column of B_e is already K-contiguous), so no per-element
     product is formed on CUDA cores before the MMA.
-  * Precision: hi = value rounded to nearest TF32, lo = the remainder (both exact TF32
-    inputs); hi*hi accumulates in one TMEM accumulator, hi*lo + lo*hi in a second, summed
-    in FP32 in the epilogue.
+  * Precision: hi = value rounded to nearest TF32, lo = the remainder (the tensor core
+    reads its TF32 part); the three products hi*hi, hi*lo and lo*hi accumulate in one TMEM
+    accumulator (plan option acc=1) or hi*hi apart from the cross terms (acc=2), summed in
+    FP32 in the epilogue.
   * Epilogue: lane i of a stacked block holds row i of W_t for every flat column; each
     producer reads its row of one element's P columns (tcgen05.ld), sums the two
     accumulators and applies R_{e,t} with its compile-time pattern unrolled. The two
     lane halves (terms 0 / 1) combine through the shared staging buffer, which is written
     back with one bulk store (cp.async.bulk, shared -> global) when the output is strided,
     aligned and unmasked, else element by element.
-  * Pipelining: two B tiles and two accumulator sets (TMEM columns
-    2 buffers x blocks x 2 accumulators x N <= 512), so the tensor cores work on tile n
-    while the producers split tile n+1 and run the epilogue of tile n-1. Every mbarrier
+  * Pipelining: two accumulator sets (TMEM columns 2 x blocks x accumulators x N <= 512)
+    and one or two B tiles (plan option bbuf), so the tensor cores work on tile n while the
+    producers run the epilogue of tile n-1 (and, with two B tiles, split tile n+1). The
+    tile is the largest element count that fits TMEM and shared memory. Every mbarrier
     wait is bounded (error word `tfb_kernel_error_<name>`), named barriers are taken
     uniformly by all producers.
 """
