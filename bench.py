@@ -419,10 +419,11 @@ def impl_ours(args, rank, world, dist):
   device = torch.device('cuda', torch.cuda.current_device())
   n = args.elements
   variants = ['plain'] if args.variant == 'plain' else (
-    [args.variant] if args.variant != 'auto' else ['tf32x3', 'fp16x3', 'plain', 'tf32x3_form_b', 'tf32x3_form_b2'])
+    [args.variant] if args.variant != 'auto' else ['tf32x3', 'fp16x3', 'plain', 'tf32x3_form_b', 'tf32x3_form_b2', 'tf32x3_form_b_ws'])
   opts_of = {'plain': {}, 'tf32x3': {'precision': 'tf32x3'}, 'fp16x3': {'precision': 'fp16x3'},
              'tf32x3_form_b': {'precision': 'tf32x3', 'variant': {'form': 'b'}},
              'tf32x3_form_b2': {'precision': 'tf32x3', 'variant': {'form': 'b', 'bbuf': 2}},
+             'tf32x3_form_b_ws': {'precision': 'tf32x3', 'variant': {'form': 'b', 'ws': 1}},
              'bf16x3': {'precision': 'bf16x3'}, 'generic': {'variant': {'strategy': 'generic'}}}
   results = {}
   stream = torch.cuda.current_stream()

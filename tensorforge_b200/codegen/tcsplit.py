@@ -156,10 +156,14 @@ def plan(chain, shape, precision, variant):
   if precision == 'tf32x3' and form == 'b':
     # operand form B (codegen/tcsplit_b.py) when every term reads the same per-element input
     from .tcsplit_b import layout_b
-    acc, bbuf = int(variant.get('acc', 1)), int(variant.get('bbuf', 1))
-    lb = layout_b(shape, acc, bbuf, variant.get('te'))
+    acc, bbuf, ws = int(variant.get('acc', 1)), int(variant.get('bbuf', 1)), int(variant.get('ws', 0))
+    if ws:
+      bbuf = 2   # the split team runs ahead of the tensor cores
+    lb = layout_b(shape, acc, bbuf, variant.get('te'), ws)
     if lb is not None:
       params = {'precision': precision, 'form': 'b', 'acc': acc, 'bbuf': bbuf, 'te': lb['te']}
+      if ws:
+        params['ws'] = 1
       return Plan('tcsplit', params, max(lb['total'], 120 * 1024), 32 * (4 * H_GROUPS + 1),
                   note=f'form B: M={shape.M} N={shape.N} terms={len(shape.terms)} tile={lb["te"]} smem={lb["total"]}')
     if variant.get('form') == 'b':

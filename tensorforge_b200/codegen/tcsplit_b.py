@@ -74,7 +74,7 @@ def blocks_of(nterms):
   return None
 
 
-def _sizes(shape, te, acc, bbuf):
+def _sizes(shape, te, acc, bbuf, nrb=2):
   terms = shape.terms
   B = terms[0].B
   K, P, M, N = terms[0].K, terms[0].P, shape.M, shape.N
@@ -98,7 +98,7 @@ def _sizes(shape, te, acc, bbuf):
   off_raw = off
   off += _pad(te * vol_b * 4, 128)
   off_r = off
-  off += _pad(2 * r_vals * 4, 128)
+  off += _pad(nrb * r_vals * 4, 128)
   off_out = off
   off += _pad(te * vol_o * 4, 128)
   off_bar = off
@@ -107,10 +107,10 @@ def _sizes(shape, te, acc, bbuf):
   return dict(te=te, n_mma=n_mma, kpad=kpad, K=K, P=P, M=M, N=N, blocks=blocks, a_bytes=a_bytes,
               b_bytes=b_bytes, vol_b=vol_b, r_off=r_off, r_vals=r_vals, vol_o=vol_o, off_a=off_a, off_b=off_b,
               off_raw=off_raw, off_r=off_r, off_out=off_out, off_bar=off_bar, total=total,
-              hsplit=(te + 1) // 2, acc=acc, bbuf=bbuf, tmem=tmem)
+              hsplit=(te + 1) // 2, acc=acc, bbuf=bbuf, tmem=tmem, nrb=nrb)
 
 
-def layout_b(shape, acc=1, bbuf=1, te=None):
+def layout_b(shape, acc=1, bbuf=1, te=None, ws=0):
   """Sizes and shared-memory offsets of form B, or None when the chain does not fit it.
 
   acc: accumulators per block (1: all three split products in one; 2: hi*hi apart from the
@@ -142,7 +142,7 @@ def layout_b(shape, acc=1, bbuf=1, te=None):
   for t_e in cands:
     if t_e < 1 or _pad(t_e * P, 16) > 256:
       continue
-    L = _sizes(shape, t_e, acc, bbuf)
+    L = _sizes(shape, t_e, acc, bbuf, 3 if ws else 2)
     if L['tmem'] <= 512 and L['total'] <= SMEM_MAX:
       return L
   return None
@@ -158,7 +158,8 @@ class _TCB:
     self.ctx = ctx
     self.base = base
     p = plan_.params
-    self.L = layout_b(shape, p.get('acc', 1), p.get('bbuf', 1), p.get('te'))
+    self.ws = int(p.get('ws', 0))
+    self.L = layout_b(shape, p.get('acc', 1), p.get('bbuf', 1), p.get('te'), self.ws)
     self.lines = []
     self.ind = 0
 
@@ -251,7 +252,8 @@ class _TCB:
     lim = self.WAIT_LIMIT
     idesc = (1 << 4) | (2 << 7) | (2 << 10) | ((n_mma >> 3) << 17) | ((128 >> 4) << 24)
     BAR_STAGE, BAR_BFULL, BAR_BFREE, BAR_DFULL, BAR_DFREE = 0, 1, 3, 5, 7
-    nbars = 9
+    BAR_RFULL, BAR_RFREE = 9, 9 + L['nrb']
+    nbars = 9 + 2 * L['nrb'] if self.ws else 9
     out = s.out
     smem = max(L['total'], 120 * 1024)
     self.plan.smem_bytes = smem
@@ -319,13 +321,20 @@ class _TCB:
       self.w(f'*reinterpret_cast<unsigned*>(tfb_smem_raw + {hi_off} + boff) = hb;')
       self.w(f'*reinterpret_cast<unsigned*>(tfb_smem_raw + {lo_off} + boff) = lb;')
       self.close()
+    # warp-specialized producers: warps 0-3 load and split (NS threads), warps 4-15 run the
+    # epilogue (NE threads); otherwise all NP producers do both
+    NS, NE = (128, NP - 128) if self.ws else (NP, NP)
     self.open('if (threadIdx.x == 0)')
-    self.w(f'tfb_tc::mbar_init(&bars[{BAR_STAGE}], {NP}u);')
+    self.w(f'tfb_tc::mbar_init(&bars[{BAR_STAGE}], {NS}u);')
     for x in range(2):
-      self.w(f'tfb_tc::mbar_init(&bars[{BAR_BFULL + x}], {NP}u);')
+      self.w(f'tfb_tc::mbar_init(&bars[{BAR_BFULL + x}], {NS}u);')
       self.w(f'tfb_tc::mbar_init(&bars[{BAR_BFREE + x}], 1u);')
       self.w(f'tfb_tc::mbar_init(&bars[{BAR_DFULL + x}], 1u);')
-      self.w(f'tfb_tc::mbar_init(&bars[{BAR_DFREE + x}], {NP}u);')
+      self.w(f'tfb_tc::mbar_init(&bars[{BAR_DFREE + x}], {NE}u);')
+    if self.ws:
+      for x in range(L['nrb']):
+        self.w(f'tfb_tc::mbar_init(&bars[{BAR_RFULL + x}], {NS}u);')
+        self.w(f'tfb_tc::mbar_init(&bars[{BAR_RFREE + x}], {NE}u);')
     self.w('asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");')
     self.close()
     self.open('if (warp == 0)')
@@ -375,7 +384,11 @@ class _TCB:
     self.close()
     self.close()
     # ---- producers
-    self._producers(NP, lim, BAR_STAGE, BAR_BFULL, BAR_BFREE, BAR_DFULL, BAR_DFREE)
+    if self.ws:
+      self._split_team(lim, BAR_STAGE, BAR_BFULL, BAR_BFREE, BAR_RFULL, BAR_RFREE)
+      self._epilogue_team(lim, BAR_DFULL, BAR_DFREE, BAR_RFULL, BAR_RFREE)
+    else:
+      self._producers(NP, lim, BAR_STAGE, BAR_BFULL, BAR_BFREE, BAR_DFULL, BAR_DFREE)
     # ---- teardown
     self.w('tfb_tc::fence_before();')
     self.w('__syncthreads();')
@@ -461,7 +474,7 @@ class _TCB:
       return '0u', 'it & 1u', 'it >= 1u', '(it - 1u) & 1u'
     return '(it & 1u)', '(it >> 1) & 1u', 'it >= 2u', '((it - 2u) >> 1) & 1u'
 
-  def _split(self, NP, bsel):
+  def _split(self, NP, bsel, tid='ptid'):
     """raw stage (column-major K x P per element) -> B tile hi / lo in canonical K-major layout;
     row n = flat column (e, m), K contiguous (a column of B_e), 4 values per item. Consecutive
     threads take consecutive rows n, so each 8-row core matrix is one conflict-free 128-byte
@@ -474,7 +487,7 @@ class _TCB:
     self.open('')
     self.w(f'unsigned char* const bh = tfb_smem_raw + {L["off_b"]} + {bsel} * {2 * L["b_bytes"]}u;')
     self.w(f'unsigned char* const bl = bh + {L["b_bytes"]}u;')
-    self.open(f'for (unsigned q = ptid; q < {nr * k4}u; q += {NP}u)')
+    self.open(f'for (unsigned q = {tid}; q < {nr * k4}u; q += {NP}u)')
     self.w(f'const unsigned l4 = q / {nr}u, n = q - l4 * {nr}u;')
     self.w(f'const unsigned ei = n / {P}u, m = n - ei * {P}u;')
     self.w('float4 x = make_float4(0.0f, 0.0f, 0.0f, 0.0f);')
@@ -632,4 +645,156 @@ class _TCB:
     self.w('const size_t ee = pe0 + ei;')
     self.w(f'if (flags == nullptr || flags[ee] != 0u) {self._elem_ptr(out, "ee")}[c] = stg[q];')
     self.close()
+    self.close()
+
+  # ------------------------------------------------------------------ warp-specialized producers
+  def _split_team(self, lim, BAR_STAGE, BAR_BFULL, BAR_BFREE, BAR_RFULL, BAR_RFREE):
+    """Warps 0-3: per tile, wait for the staged input, split it into the free B buffer, then
+    stage the next tile's input and R values (R in a ring of nrb buffers, each reloaded only
+    after the epilogue team released it)."""
+    L, b = self.L, self.base
+    NS = 128
+    nrb = L['nrb']
+    has_r = bool(L['r_off'])
+    self.open('if (warp < 4)')
+    self.w('const unsigned ptid = threadIdx.x;')
+    self.w('unsigned it = 0;')
+    self.w('bool pending = false;')
+    self.open('if (blockIdx.x < numTiles)')
+    self._load_b('(size_t)blockIdx.x', NS)
+    self.w(f'tfb_tc::cp_async_mbar_arrive(&bars[{BAR_STAGE}]);')
+    if has_r:
+      self._load_r('(size_t)blockIdx.x', 'rbase', NS)
+      self.w(f'tfb_tc::cp_async_mbar_arrive(&bars[{BAR_RFULL}]);')
+    self.w('pending = true;')
+    self.close()
+    self.open('for (size_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++it)')
+    self.w(f'if (tfb_tc::any_sync(2, {NS}, !ok)) break;')
+    self.w('const size_t ntile = tile + gridDim.x;')
+    self.w('const bool has_next = ntile < numTiles;')
+    self.w(f'if (!tfb_tc::mbar_wait(&bars[{BAR_STAGE}], it & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 70u); }}')
+    self.w('pending = false;')
+    bsel, _, free_cond, free_par = self._bbuf_exprs()
+    self.w(f'if ({free_cond} && !tfb_tc::mbar_wait(&bars[{BAR_BFREE} + {bsel}], {free_par}, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 71u); }}')
+    self._split(NS, bsel)
+    self.w('tfb_tc::fence_proxy_async();')
+    self.w(f'tfb_tc::mbar_arrive(&bars[{BAR_BFULL} + {bsel}]);')
+    self.w(f'tfb_tc::named_sync(2, {NS});   // the raw stage has been read')
+    self.open('if (has_next)')
+    self._load_b('ntile', NS)
+    self.w(f'tfb_tc::cp_async_mbar_arrive(&bars[{BAR_STAGE}]);')
+    if has_r:
+      self.w(f'const unsigned nr = (it + 1u) % {nrb}u;')
+      self.w(f'// the epilogue of tile it + 1 - {nrb} released this R buffer')
+      self.w(f'if (it + 1u >= {nrb}u && !tfb_tc::mbar_wait(&bars[{BAR_RFREE}] + nr, ((it + 1u - {nrb}u) / {nrb}u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 72u); }}')
+      self._load_r('ntile', f'(rbase + nr * {L["r_vals"]}u)', NS)
+      self.w(f'tfb_tc::cp_async_mbar_arrive(&bars[{BAR_RFULL}] + nr);')
+    self.w('pending = true;')
+    self.close()
+    self.close()
+    self.w('// loads still in flight after an abort must land before the CTA exits')
+    self.w(f'if (pending && !tfb_tc::mbar_wait(&bars[{BAR_STAGE}], it & 1u, {lim}ull)) atomicMax(&tfb_err_{b}, 73u);')
+    self.w('tfb_tc::cp_async_wait_all();')
+    self.close()
+
+  def _epilogue_team(self, lim, BAR_DFULL, BAR_DFREE, BAR_RFULL, BAR_RFREE):
+    """Warps 4-15 (three per TMEM lane quadrant): per tile, wait for its accumulators and R
+    values, apply R, release both, combine the lane halves and write the tile back."""
+    s, L, b = self.s, self.L, self.base
+    te, P, M, N = L['te'], L['P'], L['M'], L['N']
+    NE = 384
+    G3 = 3
+    nrb = L['nrb']
+    has_r = bool(L['r_off'])
+    blocks = L['blocks']
+    hs = L['hsplit']
+    per = (te + G3 - 1) // G3
+    out = s.out
+    vol_o = L['vol_o']
+    self.open('else if (warp < 16)')
+    self.w('const unsigned etid = threadIdx.x - 128u;')
+    self.w('const unsigned quad = warp & 3u, grp = (warp >> 2) - 1u;')
+    self.w('const unsigned tl = quad * 32u + lane;')
+    self.w('const unsigned half = tl >> 6, row = tl & 63u;')
+    self.w('const unsigned lane_addr = tmem + ((quad * 32u) << 16);')
+    self.w('unsigned it = 0;')
+    self.open('for (size_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++it)')
+    self.w(f'if (tfb_tc::any_sync(3, {NE}, !ok)) break;')
+    self.w('const unsigned pb = it & 1u;')
+    self.w(f'if (!tfb_tc::mbar_wait(&bars[{BAR_DFULL}] + pb, (it >> 1) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 80u); }}')
+    if has_r:
+      self.w(f'const unsigned rb = it % {nrb}u;')
+      self.w(f'if (!tfb_tc::mbar_wait(&bars[{BAR_RFULL}] + rb, (it / {nrb}u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 81u); }}')
+      self.w(f'const float* const rprev = rbase + rb * {L["r_vals"]}u;')
+    self.w('tfb_tc::fence_after();')
+    for k in range(per):
+      self.w(f'float p{k}[{N}];')
+      self.w('#pragma unroll')
+      self.w(f'for (int j = 0; j < {N}; ++j) p{k}[j] = 0.0f;')
+    for g in range(G3):
+      self.open(f'{"if" if g == 0 else "else if"} (grp == {g}u)')
+      for k in range(per):
+        e = g + k * G3
+        if e >= te:
+          continue
+        for blk, (tlo, thi, split) in enumerate(blocks):
+          if split:
+            self.open(f'if (half == {0 if e < hs else 1}u)')
+            self._term_partial(tlo, e, blk, f'p{k}')
+            self.close()
+          else:
+            self.open('if (half == 0u)')
+            self._term_partial(tlo, e, blk, f'p{k}')
+            self.close()
+            self.open('else')
+            self._term_partial(thi, e, blk, f'p{k}')
+            self.close()
+      self.close()
+    self.w('tfb_tc::fence_before();')
+    self.w(f'tfb_tc::mbar_arrive(&bars[{BAR_DFREE}] + pb);')
+    if has_r:
+      self.w(f'tfb_tc::mbar_arrive(&bars[{BAR_RFREE}] + rb);')
+    self.w(f'const size_t pe0 = tile * {te}u;')
+    self.w(f'const unsigned nvalid = (unsigned)((numElements - pe0) < {te}u ? (numElements - pe0) : {te}u);')
+    self.w('if (etid == 0) tfb_tc::bulk_wait_read();')
+    self.w(f'tfb_tc::named_sync(3, {NE});')
+    first_half1_assigns = len(s.terms) == 1
+    for phase in (0, 1):
+      self.open(f'if (half == {phase}u && row < {M}u)')
+      for k in range(per):
+        e = f'(grp + {k * G3}u)'
+        self.open(f'if ({e} < nvalid)')
+        self.w(f'float* const dst = stg + {e} * {vol_o}u + row;')
+        if phase == 0:
+          cond = '' if not blocks[0][2] else f'if ({e} < {hs}u) '
+          self.w(f'{cond}{{ ' + ' '.join(f'dst[{j * M}] = p{k}[{j}];' for j in range(N)) + ' }')
+        elif first_half1_assigns:
+          self.w(f'if ({e} >= {hs}u) {{ ' + ' '.join(f'dst[{j * M}] = p{k}[{j}];' for j in range(N)) + ' }')
+        else:
+          self.w('{ ' + ' '.join(f'dst[{j * M}] += p{k}[{j}];' for j in range(N)) + ' }')
+        self.close()
+      self.close()
+      if phase == 1:
+        self.w('tfb_tc::fence_proxy_async();   // staged values visible to the bulk store')
+      self.w(f'tfb_tc::named_sync(3, {NE});')
+    bulk_ok = out.addressing.name == 'STRIDED' and out.element_volume() == vol_o and (vol_o * 4) % 16 == 0
+    if bulk_ok:
+      self.w(f'float* const obase = {out.name} + pe0 * {out.element_volume()}u + {out.name}_extraOffset;')
+      self.w('const bool bulk = flags == nullptr && ((reinterpret_cast<uintptr_t>(obase) & 15u) == 0u);')
+      self.open('if (bulk)')
+      self.open('if (etid == 0)')
+      self.w(f'tfb_tc::bulk_store(obase, stg, nvalid * {vol_o * 4}u);')
+      self.close()
+      self.close()
+      self.open('else')
+    else:
+      self.open('')
+    self.open(f'for (unsigned q = etid; q < nvalid * {vol_o}u; q += {NE}u)')
+    self.w(f'const unsigned ei = q / {vol_o}u, c = q - ei * {vol_o}u;')
+    self.w('const size_t ee = pe0 + ei;')
+    self.w(f'if (flags == nullptr || flags[ee] != 0u) {self._elem_ptr(out, "ee")}[c] = stg[q];')
+    self.close()
+    self.close()
+    self.close()
+    self.w('if (etid == 0) tfb_tc::bulk_wait();')
     self.close()

@@ -24,6 +24,9 @@ EXTRA = [
   ('c0_gemm_strided', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b'}}),
   ('chain_o6', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b', 'acc': 2, 'bbuf': 2}}),
   ('chain_o6', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b', 'bbuf': 2}}),
+  ('chain_o6', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b', 'ws': 1}}),
+  ('c0_gemm_ptr', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b', 'ws': 1}}),
+  ('c0_gemm_strided', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b', 'ws': 1}}),
   ('c0_gemm_ptr', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b', 'acc': 2, 'bbuf': 2}}),
   ('c0_gemm_strided', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b', 'acc': 2, 'bbuf': 2}}),
   ('c0_gemm_ptr', 'float', {'precision': 'tf32x3'}),

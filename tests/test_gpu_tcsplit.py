@@ -132,9 +132,11 @@ FORM_B = {'form': 'b'}
 
 
 FORM_B_2ACC = {'form': 'b', 'acc': 2, 'bbuf': 2}
+FORM_B_WS = {'form': 'b', 'ws': 1}
 
 
-@pytest.mark.parametrize('form', [FORM_B, FORM_B_2ACC, FORM_U], ids=['formB', 'formB_2acc_2buf', 'formU'])
+@pytest.mark.parametrize('form', [FORM_B, FORM_B_2ACC, FORM_B_WS, FORM_U],
+                         ids=['formB', 'formB_2acc_2buf', 'formB_warp_specialized', 'formU'])
 @pytest.mark.parametrize('n', [1, 7, 8, 333, 4099])
 def test_chain_o6_both_operand_forms(form, n):
   """Operand form B (the per-element input as the MMA B operand, R applied in the epilogue)
@@ -144,7 +146,7 @@ def test_chain_o6_both_operand_forms(form, n):
   assert rel <= 1e-6, rel
 
 
-@pytest.mark.parametrize('form', [FORM_B, FORM_B_2ACC], ids=['formB', 'formB_2acc_2buf'])
+@pytest.mark.parametrize('form', [FORM_B, FORM_B_2ACC, FORM_B_WS], ids=['formB', 'formB_2acc_2buf', 'formB_ws'])
 @pytest.mark.parametrize('case', ['c0_gemm_ptr', 'c0_gemm_strided'])
 def test_form_b_single_term(case, form):
   """One term (the A block stacked with itself, elements split between the lane halves),
@@ -156,12 +158,13 @@ def test_form_b_single_term(case, form):
   assert rel <= 1e-6, rel
 
 
-def test_form_b_flags_and_loguniform():
-  got, ref, out, flags = _run('chain_o6', 'tf32x3', 611, use_flags=True, variant=dict(FORM_B))
+@pytest.mark.parametrize('form', [FORM_B, FORM_B_WS], ids=['formB', 'formB_ws'])
+def test_form_b_flags_and_loguniform(form):
+  got, ref, out, flags = _run('chain_o6', 'tf32x3', 611, use_flags=True, variant=dict(form))
   rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
   assert rel <= 1e-6, rel
   for e in np.nonzero(flags == 0)[0][:5]:
     s = out.starts[e]
     assert np.array_equal(got[s:s + 504], ref[s:s + 504])
-  got, ref, _, _ = _run('chain_o6', 'tf32x3', 777, dist='loguniform', variant=dict(FORM_B))
+  got, ref, _, _ = _run('chain_o6', 'tf32x3', 777, dist='loguniform', variant=dict(form))
   assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-6
