@@ -224,7 +224,8 @@ class GpuKernelGeneratorV1:
     g.register()
     cpp(self._call_site(g))
     g.generate()
-    headers = ['cuda_runtime.h', 'cstdint', 'atomic'] + context.get_vm().get_headers()
+    # everything the emitted kernels and launchers use (PRELUDE of tensorforge_b200.codegen)
+    headers = ['cuda_runtime.h', 'cstdint', 'cstddef', 'atomic', 'mutex', 'cstdio'] + context.get_vm().get_headers()
     routine_cache.addRoutine(g.get_base_name(), TensorForgeWriter(g, headers))
     return g
 
