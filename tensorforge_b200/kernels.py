@@ -41,7 +41,8 @@ EXTRA = [
   ('chain_o4_q27', 'double', {'precision': 'dmma'}),
   ('chain_o3_dense', 'double', {'precision': 'dmma'}),
   ('c0_gemm_ptr', 'float', {}),
-]
+] + [(f'kat_matmul_{v}', 'float', o) for v in ('ab', 'atb', 'abt', 'atbt')
+     for o in ({}, {'variant': {'strategy': 'generic', 'threads_per_element': 32, 'elements_per_block': 4}})]
 
 
 def make(case, fp='float', **opts):

@@ -174,6 +174,28 @@ def outer_product(ns):
   return [ns.MultilinearDescr(ns.SubTensor(D), [ns.SubTensor(a), ns.SubTensor(b)], [[0], [1]], [[0], [0]])]
 
 
+def kat_matmul(ns, trans_a=False, trans_b=False, size=32):
+  """The yateto code-generation matmul fixtures (tests/code-gen/matmul/ssm_86_Eigen:
+  kernel.cpp:9-60, subroutine.h:3-6): C = op(A) op(B) for 32x32 pointer-array operands,
+  written as the descriptor lists whose launchers have the fixtures' parameter order --
+  (C, A, B) for AB; (A, B, C) for A^T B, where yateto forms the product into a temporary
+  that is then copied to C; (A, C, B) for A B^T and A^T B^T, where A (transposed or not) is
+  first copied into a temporary."""
+  P = ns.Addressing.PTR_BASED
+  A, B, C = ns.Tensor([size, size], P), ns.Tensor([size, size], P), ns.Tensor([size, size], P)
+  ident = [[0, 1], [0, 1]]
+  sub = ns.SubTensor
+  if not trans_a and not trans_b:
+    return [ns.MultilinearDescr(sub(C), [sub(A), sub(B)], [[0, -1], [-1, 1]], ident)]
+  T = ns.Tensor([size, size], ns.Addressing.STRIDED, is_tmp=True)
+  if trans_a and not trans_b:
+    return [ns.MultilinearDescr(sub(T), [sub(A), sub(B)], [[-1, 0], [-1, 1]], ident),
+            ns.MultilinearDescr(sub(C), [sub(T)], [[0, 1]], [[0, 1]])]
+  copy = [[1, 0]] if trans_a else [[0, 1]]
+  return [ns.MultilinearDescr(sub(T), [sub(A)], copy, [[0, 1]]),
+          ns.MultilinearDescr(sub(C), [sub(T), sub(B)], [[0, -1], [1, -1]], ident)]
+
+
 CASES = {
   # name: (builder, kwargs, num_elements)
   'c0_gemm_ptr': (plain_gemm, {}, 24),
@@ -196,6 +218,10 @@ CASES = {
   'two_contractions': (two_contractions, {}, 8),
   'scalar_scaled': (scalar_scaled, {}, 8),
   'outer_product': (outer_product, {}, 8),
+  'kat_matmul_ab': (kat_matmul, {}, 1),
+  'kat_matmul_atb': (kat_matmul, {'trans_a': True}, 1),
+  'kat_matmul_abt': (kat_matmul, {'trans_b': True}, 1),
+  'kat_matmul_atbt': (kat_matmul, {'trans_a': True, 'trans_b': True}, 1),
 }
 
 
