@@ -74,13 +74,22 @@ class _ColProg:
     self.BT = plan.params['threads']
     self.LC = plan.params['chunk']
     self.asrc = plan.params.get('a_source', 'const')
+    # leading terms whose A values are constant-bank FMA operands; the rest read shared memory
+    nterms = len(shape.terms)
+    self.const_terms = {'const': nterms, 'smem': 0}.get(self.asrc, int(plan.params.get('const_terms', 0)))
+    self.term_const = [ti < self.const_terms for ti in range(nterms)]
     self.prefetch = bool(plan.params.get('prefetch', 1)) and not getattr(self, 'grouped', False)
     self.CPT = int(plan.params.get('cols', 1))
     self.TE = tile_elements(shape, self.BT, self.CPT)
     self.TC = self.TE * shape.N
     self.TCT = self.TC // self.CPT        # columns per round: thread t owns t + r * TCT
     self.kmax = max(t.K for t in shape.terms)
-    self.pitch = _pad(self.kmax, self.VEC) + self.VEC
+    # U^T rows: K + VEC values keep 16-byte row starts (vector loads) and spread the rows of
+    # a quarter-warp over the banks; an odd pitch (scalar loads) is conflict-free and smaller
+    if plan.params.get('upitch', 'vec') == 'odd':
+      self.pitch = self.kmax | 1
+    else:
+      self.pitch = _pad(self.kmax, self.VEC) + self.VEC
     self.lines = []
     self.ind = 0
 
@@ -136,18 +145,24 @@ class _ColProg:
     s = self.s
     # A storage: every term's values, in storage order, concatenated
     self.a_base = []
-    total = 0
-    for t in s.terms:
-      self.a_base.append(total)
-      total += t.A.storage_size()
-    self.a_total = total
+    ctot = stot = 0
+    for ti, t in enumerate(s.terms):
+      if self.term_const[ti]:
+        self.a_base.append(ctot)
+        ctot += t.A.storage_size()
+      else:
+        self.a_base.append(stot)
+        stot += t.A.storage_size()
+    self.a_const_total, self.a_smem_total = ctot, stot
+    self.a_total = ctot + stot
     # rounded to whole vectors: the staged R copies behind it are read as float4 / double2
     self.ubuf_vals = _pad(max(self.TC * self.pitch, self.TC * s.M), self.VEC)
     # per-tile copies of the batched R operands (read as 128-bit broadcast loads)
+    # (not needed with the prefetch stage, which holds them)
     self.r_off = {}
     r_vals = 0
     for t in s.terms:
-      if t.R is not None and t.R.kind == 'batched' and t.R.name not in self.r_off:
+      if not self.prefetch and t.R is not None and t.R.kind == 'batched' and t.R.name not in self.r_off:
         self.r_off[t.R.name] = self.ubuf_vals + r_vals
         r_vals += self.TE * _pad(t.R.storage_size(), self.VEC)
     self.work_vals = _pad(self.ubuf_vals + r_vals, self.VEC)   # ubuf + staged R, per CTA
@@ -160,7 +175,7 @@ class _ColProg:
           if op is not None and op.kind == 'batched' and op.name not in self.stage_off:
             self.stage_off[op.name] = self.work_vals + self.stage_vals
             self.stage_vals += self.TE * _pad(op.storage_size() if op.sparse else op.element_volume(), self.VEC)
-    a_smem = _pad(self.a_total, self.VEC) if self.asrc == 'smem' else 0
+    a_smem = _pad(self.a_smem_total, self.VEC) if self.a_smem_total else 0
     self.a_off = self.work_vals + self.stage_vals
     self.smem = (self.work_vals + self.stage_vals + a_smem) * self.FS
 
@@ -244,18 +259,19 @@ class _ColProg:
     kname = f'kernel_{b}'
     self._layout()
     self._header()
-    if self.asrc == 'const':
-      self.w(f'__constant__ {T} cA_{b}[{self.a_total}];')
+    if self.a_const_total:
+      self.w(f'__constant__ {T} cA_{b}[{self.a_const_total}];')
     mb = self.plan.params.get('min_blocks', 0)
     bounds = f'{BT}, {mb}' if mb else f'{BT}'
     self.w(f'__global__ void __launch_bounds__({bounds}) {kname}({", ".join(self.params(globals_))}) {{')
     self.ind += 1
     self.w('extern __shared__ __align__(16) unsigned char tfb_smem_raw[];')
     self.w(f'{T}* const ubuf = reinterpret_cast<{T}*>(tfb_smem_raw);')
-    if self.asrc == 'smem':
+    if self.a_smem_total:
       self.w(f'{T}* const sA = ubuf + {self.a_off};')
       for ti, t in enumerate(s.terms):
-        self.w(f'for (int q = threadIdx.x; q < {t.A.storage_size()}; q += {BT}) sA[{self.a_base[ti]} + q] = {t.A.name}[q];')
+        if not self.term_const[ti]:
+          self.w(f'for (int q = threadIdx.x; q < {t.A.storage_size()}; q += {BT}) sA[{self.a_base[ti]} + q] = {t.A.name}[q];')
       self.w('__syncthreads();')
     self.w(f'const size_t numTiles = (numElements + {self.TE - 1}u) / {self.TE}u;')
     if self.prefetch:
@@ -333,7 +349,7 @@ class _ColProg:
            f'  }}',
            f'  const size_t cap = device < 64 ? (size_t)occ[device] : (size_t)1024;',
            f'  if (grid.x > cap) grid.x = (unsigned)cap;']
-    if self.asrc == 'const':
+    if self.a_const_total:
       # the constant bank is one per module: refresh it on the launch stream, and order
       # launches issued from different streams after the previous launch (outside capture)
       pre += [f'  static std::mutex mu;',
@@ -347,8 +363,9 @@ class _ColProg:
               f'  if (!capturing && device < 64 && haveLast[device] && lastStream[device] != stream)',
               f'    cudaStreamWaitEvent(stream, lastEv[device], 0);']
       for ti, t in enumerate(s.terms):
-        pre.append(f'  cudaMemcpyToSymbolAsync(cA_{b}, {t.A.name}, {t.A.storage_size() * self.FS}, '
-                   f'{self.a_base[ti] * self.FS}, cudaMemcpyDeviceToDevice, stream);')
+        if self.term_const[ti]:
+          pre.append(f'  cudaMemcpyToSymbolAsync(cA_{b}, {t.A.name}, {t.A.storage_size() * self.FS}, '
+                     f'{self.a_base[ti] * self.FS}, cudaMemcpyDeviceToDevice, stream);')
       pre += [f'  {kname}<<<grid, block, {self.smem}, stream>>>({", ".join(args)});',
               f'  CHECK_ERR;',
               f'  if (!capturing && device < 64) {{',
@@ -441,7 +458,7 @@ class _ColProg:
     loaded = set()
 
     def a_operand(pos):
-      if self.asrc == 'const':
+      if self.term_const[ti]:
         return f'cA_{b}[{self.a_base[ti] + pos}]'
       g = self.a_base[ti] + pos
       v = g // VEC
@@ -456,10 +473,11 @@ class _ColProg:
       for r in R:
         u, uc = f'u{sfx(r)}', f'ucol{sfx(r)}'
         self.w(f'{T} {u}[{n}];')
-        for v in range(n // VEC):
+        nv = n // VEC if self.pitch % VEC == 0 else 0
+        for v in range(nv):
           self.w(f'{{ const {VT} x = *reinterpret_cast<const {VT}*>({uc} + {l0 + v * VEC}); '
                  + ' '.join(f'{u}[{v * VEC + c}] = x.{comps[c]};' for c in range(VEC)) + ' }')
-        for i in range(n // VEC * VEC, n):
+        for i in range(nv * VEC, n):
           self.w(f'{u}[{i}] = {uc}[{l0 + i}];')
       for l in range(l0, l0 + n):
         for (i, pos) in cols[l][1]:

@@ -37,6 +37,10 @@ EXTRA = [
   ('chain_o6', 'float', {'precision': 'bf16x3', 'variant': {'pipe': 1}}),
   ('chain_o6', 'double', {}),
   ('chain_o6', 'double', {'variant': {'strategy': 'colprog'}}),
+  ('chain_o6', 'float', {'variant': {'strategy': 'colprog', 'a_source': 'mixed', 'const_terms': 1, 'upitch': 'odd',
+                                     'min_blocks': 3}}),
+  ('c0_gemm_ptr', 'float', {'variant': {'strategy': 'colprog', 'a_source': 'mixed', 'const_terms': 1, 'upitch': 'odd',
+                                        'min_blocks': 3}}),
   ('chain_o6', 'double', {'precision': 'dmma'}),
   ('chain_o4_q27', 'double', {'precision': 'dmma'}),
   ('chain_o3_dense', 'double', {'precision': 'dmma'}),

@@ -189,43 +189,76 @@ COLPROG_MAX_FMAS = 6144
 COLPROG_CONST_A = 4096
 
 
+# Variant 'mixed' (not a default): the leading terms whose A values fit this budget stay
+# constant-bank FMA operands and the rest move to shared memory. With an odd U pitch it
+# brings the order-6 chain's CTA to 72 KB of shared memory and 167 registers, three CTAs per
+# SM instead of two -- measured slower (2.61e8 against 2.71e8 el/s), as were the other
+# three-CTA forms (2.49e8-2.65e8).
+COLPROG_CONST_MIXED = 2048
+
+
 def colprog_plan(chain, shape: LeftChain, fp_size, variant):
   from ..codegen.colprog import tile_elements
   threads = variant.get('threads', 128)
   chunk = variant.get('chunk', 16)
-  a_total = sum(t.A.storage_size() for t in shape.terms)
-  a_source = variant.get('a_source', 'const' if a_total <= COLPROG_CONST_A else 'smem')
+  sizes = [t.A.storage_size() for t in shape.terms]
+  a_total = sum(sizes)
+  if 'a_source' in variant:
+    a_source = variant['a_source']
+  elif a_total <= COLPROG_CONST_A:
+    a_source = 'const'
+  else:
+    a_source = 'smem'
+  const_terms = int(variant.get('const_terms', 0))
+  if a_source == 'mixed' and 'const_terms' not in variant:
+    acc = 0
+    for n in sizes:
+      if acc + n > COLPROG_CONST_MIXED:
+        break
+      acc += n
+      const_terms += 1
+    if const_terms == 0:
+      a_source = 'smem'
   vec = 4 if fp_size == 4 else 2
   chunk = max(vec, (chunk + vec - 1) // vec * vec)
   if shape.M > 128 or shape.N > threads:
     return None
-  if sum(t.A.storage_size() for t in shape.terms) > COLPROG_MAX_FMAS:
+  if a_total > COLPROG_MAX_FMAS:
     return None
   cols = int(variant.get('cols', 1))
   te = tile_elements(shape, threads, cols)
   kmax = max(t.K for t in shape.terms)
-  pitch = (kmax + vec - 1) // vec * vec + vec
-  a_vals = sum(t.A.storage_size() for t in shape.terms)
-  if a_source == 'const' and a_vals * fp_size > 48 * 1024:
+  upitch = variant.get('upitch', 'odd' if a_source == 'mixed' else 'vec')
+  pitch = (kmax | 1) if upitch == 'odd' else (kmax + vec - 1) // vec * vec + vec
+  if a_source == 'const' and a_total * fp_size > 48 * 1024:
     a_source = 'smem'
+  n_const = {'const': len(sizes), 'smem': 0}.get(a_source, const_terms)
+  a_smem_vals = sum(sizes[n_const:])
+  prefetch = int(variant.get('prefetch', 1))
   smem = max(te * shape.N * pitch, te * shape.N * shape.M) * fp_size
-  smem += sum(te * ((t.R.storage_size() + vec - 1) // vec * vec) for t in shape.terms
-              if t.R is not None and t.R.kind == 'batched') * fp_size
-  if a_source == 'smem':
-    smem += (a_vals + vec) * fp_size
+  r_staged = sum(te * ((t.R.storage_size() + vec - 1) // vec * vec) for t in shape.terms
+                 if t.R is not None and t.R.kind == 'batched') * fp_size
+  if a_smem_vals:
+    smem += (a_smem_vals + vec) * fp_size
+  stage = sum(te * ((op.storage_size() if op.sparse else op.element_volume()) + vec - 1) // vec * vec
+              for op in {id(o): o for t in shape.terms for o in (t.B, t.R)
+                         if o is not None and o.kind == 'batched'}.values()) * fp_size
+  if not prefetch or smem + stage > SMEM_LIMIT:
+    prefetch = 0
+    smem += r_staged
+  else:
+    smem += stage
   if smem > SMEM_LIMIT:
     return None
-  prefetch = int(variant.get('prefetch', 1))
-  if prefetch:
-    smem += sum(te * ((op.storage_size() if op.sparse else op.element_volume()) + vec - 1) // vec * vec
-                for op in {id(o): o for t in shape.terms for o in (t.B, t.R)
-                           if o is not None and o.kind == 'batched'}.values()) * fp_size
-    if smem > SMEM_LIMIT:
-      prefetch = 0
   # __launch_bounds__(128, 2) measured 4-5 % faster on the order-6 chain at every chunk size
   # (2.60e8 -> 2.70e8 el/s at chunk 16); 256-thread CTAs gain nothing from it
-  params = {'threads': threads, 'chunk': chunk, 'min_blocks': variant.get('min_blocks', 2 if threads == 128 else 0),
+  default_mb = 2 if threads == 128 else 0
+  params = {'threads': threads, 'chunk': chunk, 'min_blocks': variant.get('min_blocks', default_mb),
             'a_source': a_source, 'prefetch': prefetch}
+  if a_source == 'mixed':
+    params['const_terms'] = n_const
+  if upitch != 'vec':
+    params['upitch'] = upitch
   if cols != 1:
     params['cols'] = cols
   return Plan('colprog', params,

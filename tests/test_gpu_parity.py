@@ -97,6 +97,7 @@ COLPROG_VARIANTS = [
   {'strategy': 'colprog', 'a_source': 'smem'},
   {'strategy': 'colprog', 'a_source': 'smem', 'cols': 2},
   {'strategy': 'colprog', 'a_source': 'const', 'prefetch': 0, 'threads': 256},
+  {'strategy': 'colprog', 'a_source': 'mixed', 'const_terms': 1, 'upitch': 'odd', 'min_blocks': 3},
 ]
 
 
