@@ -39,7 +39,7 @@ releasing its tensor memory.
 
 Producer pipelines (plan option `pipe`):
   2 (default when it fits in shared memory): one input stage, filled by one bulk copy
-    (cp.async.bulk global -> shared, no multicast) per contiguous, 16-byte aligned B block
+    (cp.async.bulk global -> this CTA's shared memory) per contiguous, 16-byte aligned B block
     and cp.async for the R blocks, completion tracked by a stage mbarrier (expect_tx bytes
     plus one cp.async arrival per producer); one U pass computes U_t for every term (B's
     row loaded once) into one transposition buffer per term; the previous tile's output
@@ -289,7 +289,7 @@ __device__ __forceinline__ void bulk_store(void* gdst, const void* ssrc, unsigne
                :: "l"(gdst), "r"(smem_u32(ssrc)), "r"(bytes) : "memory");
   asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 }
-// global -> shared bulk copy (no multicast), completion counted in bytes on `bar`
+// global -> this CTA's shared memory bulk copy, completion counted in bytes on `bar`
 __device__ __forceinline__ void bulk_load(void* sdst, const void* gsrc, unsigned bytes, uint64_t* bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                :: "r"(smem_u32(sdst)), "l"(gsrc), "r"(bytes), "r"(smem_u32(bar)) : "memory");
