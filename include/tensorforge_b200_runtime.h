@@ -1,7 +1,8 @@
 // Entry points of the native runtime library libtfb200_runtime.so (built from
 // tensorforge_b200/csrc/*.cu). None of them has a counterpart in the reference, which has
-// no autotuner and records no rooflines: they back the learned cost model of the
-// autotuner and the measured roofline denominators.
+// no autotuner, records no rooflines and takes device buffers only: they back the learned
+// cost model of the autotuner, the measured roofline denominators and the transfers of
+// host-resident batches.
 //
 // Every function is asynchronous on `stream` (a cudaStream_t; nullptr = legacy default
 // stream), allocates nothing, and returns the cudaError_t of its launch (0 = success).
@@ -35,6 +36,14 @@ int tfb_mlp_loss(const float *Y, const float *T, int B, float *out, void *stream
 // One Adam step (bias-corrected with `step` >= 1) on n parameters; m, v are the moments.
 int tfb_mlp_adam(float *params, const float *grads, float *m, float *v, int n, float lr, float b1, float b2,
                  float eps, int step, void *stream);
+
+// ---- host-resident batches
+// 2D copy: `rows` rows of `row_bytes` bytes, consecutive rows `src_pitch` / `dst_pitch` bytes
+// apart; host -> device when to_device != 0, else device -> host. Host memory should be
+// pinned for the copy to be asynchronous. Returns cudaErrorInvalidValue when a row is wider
+// than a pitch.
+int tfb_copy_rows_async(void *dst, size_t dst_pitch, const void *src, size_t src_pitch, size_t row_bytes,
+                        size_t rows, int to_device, void *stream);
 
 #ifdef __cplusplus
 }
