@@ -282,6 +282,17 @@ def extra_workloads(stream, short=False):
                            'roofline': {'fp32_bound_el_s': fp32 / (flops / n), 'hbm_bound_el_s': hbm / bytes_el,
                                         'frac_of_tighter': (n / (ms / 1e3)) / min(fp32 / (flops / n), hbm / bytes_el),
                                         'bytes_per_element': bytes_el, 'flops_per_element': flops / n}}
+    if n >= 1000000:
+      # the same GEMM on the tensor cores (TF32x3, both operand forms; parity in the GPU tests)
+      tc = {}
+      for label, variant in (('tf32x3', None), ('tf32x3_form_b', {'form': 'b'})):
+        gt = make('c0_gemm_ptr', 'float', precision='tf32x3', **({'variant': variant} if variant else {}))
+        kt = compile_generator(gt)
+        total, per = time_launches(lambda: kt(**kw), stream, 10, 3)
+        mt = sum(per) / len(per)
+        tc[label] = {'elements_per_s': n / (mt / 1e3), 'plan': gt.get_plan().key(),
+                     'frac_hbm': (n / (mt / 1e3)) / (hbm / bytes_el)}
+      out[f'c0_gemm_{n}']['tensor_cores'] = tc
   # config 3: mixed shapes, one persistent launch over a work table, replayed from a CUDA graph
   from tensorforge_b200.kernels import grouped_catalogue
   gk = dict(grouped_catalogue())['bench_c3']
