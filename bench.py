@@ -283,9 +283,10 @@ def extra_workloads(stream, short=False):
                                         'frac_of_tighter': (n / (ms / 1e3)) / min(fp32 / (flops / n), hbm / bytes_el),
                                         'bytes_per_element': bytes_el, 'flops_per_element': flops / n}}
     if n >= 1000000:
-      # the same GEMM on the tensor cores (TF32x3, both operand forms; parity in the GPU tests)
+      # the same GEMM on the tensor cores (TF32x3: operand form B, the default for one term,
+      # and form U; parity in the GPU tests)
       tc = {}
-      for label, variant in (('tf32x3', None), ('tf32x3_form_b', {'form': 'b'})):
+      for label, variant in (('tf32x3', None), ('tf32x3_form_u', {'form': 'u'})):
         gt = make('c0_gemm_ptr', 'float', precision='tf32x3', **({'variant': variant} if variant else {}))
         kt = compile_generator(gt)
         total, per = time_launches(lambda: kt(**kw), stream, 10, 3)

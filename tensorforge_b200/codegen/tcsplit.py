@@ -149,10 +149,17 @@ def smem_plan_v2(shape, precision):
 def plan(chain, shape, precision, variant):
   if precision not in KSTEP:
     return None
-  # operand form B (codegen/tcsplit_b.py) is opt-in (variant {'form': 'b'}): measured on the
-  # order-6 chain at 3.0e8 (13-element tiles, one B buffer) and 3.7e8 el/s (8-element tiles,
-  # two B buffers) against 4.8e8 for form U below
-  form = variant.get('form', 'u')
+  # operand form B (codegen/tcsplit_b.py): the default for single-term chains (a plain GEMM
+  # per element: 3.75e8 against 2.59e8 el/s for form U on 1M 56x56 x 56x9 pointer-array
+  # GEMMs), opt-in otherwise (variant {'form': 'b'}): on the order-6 chain it measured 3.0e8
+  # (13-element tiles, one B buffer) and 3.7e8 el/s (8-element tiles, two B buffers) against
+  # 4.8e8 for form U below
+  if 'form' in variant:
+    form = variant['form']
+  elif 'pipe' in variant or 'chunk' in variant:
+    form = 'u'
+  else:
+    form = 'b' if len(shape.terms) == 1 else 'u'
   if precision == 'tf32x3' and form == 'b':
     # operand form B (codegen/tcsplit_b.py) when every term reads the same per-element input
     from .tcsplit_b import layout_b
