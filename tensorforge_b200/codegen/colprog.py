@@ -200,20 +200,37 @@ class _ColProg:
       vp = _pad(vals, VEC)
       self.open('')
       self.w(f'const size_t pe0 = ({tile_expr}) * {self.TE}u;')
-      if vals % VEC == 0:
+      small = 'copy8' if FS == 8 else 'copy4'
+      if op.addressing.name == 'PTR_BASED':
+        # one element per warp at a time: its pointer is loaded once, not once per chunk
+        self.open(f'for (unsigned ei = threadIdx.x >> 5; ei < {self.TE}u; ei += {BT // 32}u)')
+        self.w('const size_t ee = pe0 + ei;')
+        self.w('if (ee >= numElements) break;')
+        self.w(f'const {T}* const sbase = {self._elem_ptr(op, "ee")};')
+        self.w(f'{T}* const dbase = ubuf + {off} + ei * {vp}u;')
+        if vals % VEC == 0:
+          self.w('const bool al = (reinterpret_cast<uintptr_t>(sbase) & 15u) == 0u;')
+          self.open(f'for (unsigned c = threadIdx.x & 31u; c < {vals // VEC}u; c += 32u)')
+          self.w(f'const {T}* src = sbase + {VEC}u * c;')
+          self.w(f'{T}* dst = dbase + {VEC}u * c;')
+          self.w('if (al) tfb_cp::copy16(dst, src);')
+          self.w('else { ' + ' '.join(f'tfb_cp::{small}(dst + {i}, src + {i});' for i in range(VEC)) + ' }')
+          self.close()
+        else:
+          self.w(f'for (unsigned c = threadIdx.x & 31u; c < {vals}u; c += 32u) tfb_cp::{small}(dbase + c, sbase + c);')
+        self.close()
+      elif vals % VEC == 0:
         self.open(f'for (unsigned q = threadIdx.x; q < {self.TE * vals // VEC}u; q += {BT}u)')
         self.w(f'const unsigned ei = q / {vals // VEC}u, c = q - ei * {vals // VEC}u;')
         self.w('const size_t ee = pe0 + ei;')
         self.open('if (ee < numElements)')
         self.w(f'const {T}* src = {self._elem_ptr(op, "ee")} + {VEC}u * c;')
         self.w(f'{T}* dst = ubuf + {off} + ei * {vp}u + {VEC}u * c;')
-        small = 'copy8' if FS == 8 else 'copy4'
         self.w('if ((reinterpret_cast<uintptr_t>(src) & 15u) == 0u) tfb_cp::copy16(dst, src);')
         self.w('else { ' + ' '.join(f'tfb_cp::{small}(dst + {i}, src + {i});' for i in range(VEC)) + ' }')
         self.close()
         self.close()
       else:
-        small = 'copy8' if FS == 8 else 'copy4'
         self.open(f'for (unsigned q = threadIdx.x; q < {self.TE * vals}u; q += {BT}u)')
         self.w(f'const unsigned ei = q / {vals}u, c = q - ei * {vals}u;')
         self.w('const size_t ee = pe0 + ei;')

@@ -649,6 +649,27 @@ class _TC:
     vp = _pad(vals, 4)
     self.open('')
     self.w(f'const size_t pe0 = ({tile_expr}) * {te}u;')
+    if op.addressing.name == 'PTR_BASED':
+      # one element per warp at a time: its pointer is loaded once, not once per chunk
+      self.open(f'for (unsigned ei = ptid >> 5; ei < {te}u; ei += {NP // 32}u)')
+      self.w('const size_t ee = pe0 + ei;')
+      self.w('if (ee >= numElements) break;')
+      self.w(f'const float* const sbase = {self._elem_ptr(op, "ee")};')
+      self.w(f'float* const dbase = {buf} + {off} + ei * {vp}u;')
+      if vals % 4 == 0:
+        self.w('const bool al = (reinterpret_cast<uintptr_t>(sbase) & 15u) == 0u;')
+        self.open(f'for (unsigned c4 = ptid & 31u; c4 < {vals // 4}u; c4 += 32u)')
+        self.w('const float* src = sbase + 4u * c4;')
+        self.w('float* dst = dbase + 4u * c4;')
+        self.w('if (al) tfb_tc::cp_async16(dst, src);')
+        self.w('else { tfb_tc::cp_async4(dst, src); tfb_tc::cp_async4(dst + 1, src + 1); '
+               'tfb_tc::cp_async4(dst + 2, src + 2); tfb_tc::cp_async4(dst + 3, src + 3); }')
+        self.close()
+      else:
+        self.w(f'for (unsigned c = ptid & 31u; c < {vals}u; c += 32u) tfb_tc::cp_async4(dbase + c, sbase + c);')
+      self.close()
+      self.close()
+      return
     if vals % 4 == 0:
       self.open(f'for (unsigned q = ptid; q < {te * vals // 4}u; q += {NP}u)')
       self.w(f'const unsigned ei = q / {vals // 4}u, c4 = q - ei * {vals // 4}u;')

@@ -196,12 +196,36 @@ class _TCB:
       return f'({op.name}[{e}] + {op.name}_extraOffset)'
     return f'{op.name}'
 
-  def _copy(self, op, vals, dst, tile_expr, NP):
-    """cp.async `vals` values per element of tile `tile_expr` to `dst` + ei * pad4(vals)."""
+  def _copy(self, op, vals, dst, tile_expr, NP, tid='ptid'):
+    """cp.async `vals` values per element of tile `tile_expr` to `dst` + ei * pad4(vals).
+
+    Pointer-array operands are copied one element per warp at a time, so the element's
+    pointer is loaded once per warp instead of once per 16-byte chunk."""
     te = self.L['te']
     vp = _pad(vals, 4)
     self.open('')
     self.w(f'const size_t ce0 = ({tile_expr}) * {te}u;')
+    if op.addressing.name == 'PTR_BASED':
+      nw = NP // 32
+      self.open(f'for (unsigned ei = ({tid}) >> 5; ei < {te}u; ei += {nw}u)')
+      self.w('const size_t ee = ce0 + ei;')
+      self.w('if (ee >= numElements) break;')
+      self.w(f'const float* const sbase = {self._elem_ptr(op, "ee")};')
+      self.w(f'float* const dbase = {dst} + ei * {vp}u;')
+      if vals % 4 == 0:
+        self.w('const bool al = (reinterpret_cast<uintptr_t>(sbase) & 15u) == 0u;')
+        self.open(f'for (unsigned c4 = ({tid}) & 31u; c4 < {vals // 4}u; c4 += 32u)')
+        self.w('const float* src = sbase + 4u * c4;')
+        self.w('float* dst = dbase + 4u * c4;')
+        self.w('if (al) tfb_tc::cp_async16(dst, src);')
+        self.w('else { tfb_tc::cp_async4(dst, src); tfb_tc::cp_async4(dst + 1, src + 1); '
+               'tfb_tc::cp_async4(dst + 2, src + 2); tfb_tc::cp_async4(dst + 3, src + 3); }')
+        self.close()
+      else:
+        self.w(f'for (unsigned c = ({tid}) & 31u; c < {vals}u; c += 32u) tfb_tc::cp_async4(dbase + c, sbase + c);')
+      self.close()
+      self.close()
+      return
     if vals % 4 == 0:
       self.open(f'for (unsigned q = ptid; q < {te * vals // 4}u; q += {NP}u)')
       self.w(f'const unsigned ei = q / {vals // 4}u, c4 = q - ei * {vals // 4}u;')
@@ -220,6 +244,17 @@ class _TCB:
       self.w('const size_t ee = ce0 + ei;')
       self.w(f'if (ee < numElements) tfb_tc::cp_async4({dst} + ei * {vp}u + c, {self._elem_ptr(op, "ee")} + c);')
       self.close()
+    self.close()
+
+  def _store_elements(self, out, vol_o, tid, nthreads):
+    """Staged tile -> the output, one element per warp (its pointer and flag read once),
+    skipping masked elements."""
+    nw = nthreads // 32
+    self.open(f'for (unsigned ei = ({tid}) >> 5; ei < nvalid; ei += {nw}u)')
+    self.w('const size_t ee = pe0 + ei;')
+    self.w('if (flags != nullptr && flags[ee] == 0u) continue;')
+    self.w(f'float* const obase_e = {self._elem_ptr(out, "ee")};')
+    self.w(f'for (unsigned c = ({tid}) & 31u; c < {vol_o}u; c += 32u) obase_e[c] = stg[ei * {vol_o}u + c];')
     self.close()
 
   def _load_b(self, tile_expr, NP):
@@ -640,11 +675,7 @@ class _TCB:
       self.open('else')
     else:
       self.open('')
-    self.open(f'for (unsigned q = ptid; q < nvalid * {vol_o}u; q += {NP}u)')
-    self.w(f'const unsigned ei = q / {vol_o}u, c = q - ei * {vol_o}u;')
-    self.w('const size_t ee = pe0 + ei;')
-    self.w(f'if (flags == nullptr || flags[ee] != 0u) {self._elem_ptr(out, "ee")}[c] = stg[q];')
-    self.close()
+    self._store_elements(out, vol_o, 'ptid', NP)
     self.close()
 
   # ------------------------------------------------------------------ warp-specialized producers
@@ -789,11 +820,7 @@ class _TCB:
       self.open('else')
     else:
       self.open('')
-    self.open(f'for (unsigned q = etid; q < nvalid * {vol_o}u; q += {NE}u)')
-    self.w(f'const unsigned ei = q / {vol_o}u, c = q - ei * {vol_o}u;')
-    self.w('const size_t ee = pe0 + ei;')
-    self.w(f'if (flags == nullptr || flags[ee] != 0u) {self._elem_ptr(out, "ee")}[c] = stg[q];')
-    self.close()
+    self._store_elements(out, vol_o, 'etid', NE)
     self.close()
     self.close()
     self.w('if (etid == 0) tfb_tc::bulk_wait();')

@@ -27,6 +27,8 @@ EXTRA = [
   ('chain_o6', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b', 'ws': 1}}),
   ('c0_gemm_ptr', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b', 'ws': 1}}),
   ('c0_gemm_strided', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b', 'ws': 1}}),
+  ('c0_gemm_ptr', 'float', {'precision': 'tf32x3', 'variant': {'form': 'u'}}),
+  ('c0_gemm_strided', 'float', {'precision': 'tf32x3', 'variant': {'form': 'u'}}),
   ('c0_gemm_ptr', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b', 'acc': 2, 'bbuf': 2}}),
   ('c0_gemm_strided', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b', 'acc': 2, 'bbuf': 2}}),
   ('c0_gemm_ptr', 'float', {'precision': 'tf32x3'}),

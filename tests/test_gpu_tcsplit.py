@@ -146,13 +146,13 @@ def test_chain_o6_both_operand_forms(form, n):
   assert rel <= 1e-6, rel
 
 
-@pytest.mark.parametrize('form', [FORM_B, FORM_B_2ACC, FORM_B_WS], ids=['formB', 'formB_2acc_2buf', 'formB_ws'])
+@pytest.mark.parametrize('form', [FORM_B, FORM_B_2ACC, FORM_B_WS, FORM_U], ids=['formB', 'formB_2acc_2buf', 'formB_ws', 'formU'])
 @pytest.mark.parametrize('case', ['c0_gemm_ptr', 'c0_gemm_strided'])
 def test_form_b_single_term(case, form):
   """One term (the A block stacked with itself, elements split between the lane halves),
   pointer-array and strided operands, no R."""
   from tensorforge_b200.kernels import make
-  assert make(case, 'float', precision='tf32x3', variant=dict(form)).get_plan().params.get('form') == 'b'
+  assert make(case, 'float', precision='tf32x3', variant=dict(form)).get_plan().params.get('form', 'u') == form['form']
   got, ref, _, _ = _run(case, 'tf32x3', 1001, variant=dict(form))
   rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
   assert rel <= 1e-6, rel
