@@ -14,7 +14,7 @@ index box; both kinds can be mixed in one descriptor list.
 """
 from typing import List
 from ..common.exceptions import GenerationError
-from ..common.basic_types import DataFlowDirection, Addressing
+from ..common.basic_types import DataFlowDirection, Addressing, FloatingPointType  # noqa: F401 (re-exported)
 from ..common.matrix.tensor import Tensor, SubTensor
 
 
