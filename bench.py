@@ -175,6 +175,42 @@ def time_launches(fn, stream, steps, warmup, dist=None):
   return t0.elapsed_time(t1), per
 
 
+def link_bound(h2d_bytes, d2h_bytes, steps=3):
+  """Host<->device link bound of one end-to-end step: `h2d_bytes` from pinned host memory
+  and `d2h_bytes` back to pinned host memory, each as one contiguous copy, both directions
+  at once on two streams and each direction alone (best of `steps`, ms)."""
+  import torch
+  hin = torch.empty(h2d_bytes, dtype=torch.uint8, pin_memory=True)
+  din = torch.empty(h2d_bytes, dtype=torch.uint8, device='cuda')
+  hout = torch.empty(d2h_bytes, dtype=torch.uint8, pin_memory=True)
+  dout = torch.zeros(d2h_bytes, dtype=torch.uint8, device='cuda')
+  s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+  cur = torch.cuda.current_stream()
+
+  def run(do_in, do_out):
+    best = None
+    for _ in range(steps + 1):
+      torch.cuda.synchronize()
+      t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+      t0.record(cur)
+      for on, st, dst, src in ((do_in, s_in, din, hin), (do_out, s_out, hout, dout)):
+        if on:
+          st.wait_event(t0)
+          with torch.cuda.stream(st):
+            dst.copy_(src, non_blocking=True)
+          cur.wait_stream(st)
+      t1.record(cur)
+      torch.cuda.synchronize()
+      ms = t0.elapsed_time(t1)
+      best = ms if best is None else min(best, ms)
+    return best
+
+  run(True, True)
+  duplex, h2d_ms, d2h_ms = run(True, True), run(True, False), run(False, True)
+  return {'duplex_ms': duplex, 'h2d_alone_gbs': h2d_bytes / h2d_ms / 1e6, 'd2h_alone_gbs': d2h_bytes / d2h_ms / 1e6,
+          'duplex_h2d_gbs': h2d_bytes / duplex / 1e6, 'duplex_d2h_gbs': d2h_bytes / duplex / 1e6}
+
+
 # ----------------------------------------------------------------------------- CPU baseline
 
 def _cpu_bench(args_list):
@@ -549,6 +585,9 @@ def impl_ours(args, rank, world, dist):
     extra_out.setdefault('variants', {})[name] = {
       'elements_per_s': n / (sum(r['launch_ms']) / len(r['launch_ms']) / 1e3), 'plan': r['plan'],
       'rel_l2': r['accuracy']['rel_l2'], 'max_abs': r['accuracy']['max_abs']}
+  # the link bound of the end-to-end step (contiguous copies of the same byte counts)
+  link = link_bound(h2d, d2h)
+  link['frac'] = link['duplex_ms'] / e_ms
   cpu = reference_cpu() if (world == 1 and not args.no_cpu) else None
   extras = extra_workloads(stream, short=args.no_cpu) if (world == 1 and not args.no_extras) else None
   line = {
@@ -562,7 +601,8 @@ def impl_ours(args, rank, world, dist):
     'roofline': roofline,
     'cpu_baseline': cpu,
     'e2e': {'value': world * n / (e_ms / 1e3), 'unit': 'elements/s', 'h2d_bytes_per_step': h2d,
-            'd2h_bytes_per_step': d2h, 'api': 'runtime.pipeline.HostPipeline (16 slices, 3 streams)'},
+            'd2h_bytes_per_step': d2h, 'api': 'runtime.pipeline.HostPipeline (16 slices, 3 streams)',
+            'link_bound': link},
     'gpu_launches': args.steps,
     'clocks': clocks.summary(),
   }

@@ -57,8 +57,9 @@ def emit_launcher(proto, launch):
   lines.append('  cudaStream_t stream = (streamPtr != nullptr) ? static_cast<cudaStream_t>(streamPtr) : 0;')
   if pre:
     lines.append(pre)
-  lines.append(f'  {kname}<<<grid, block, {smem}, stream>>>({", ".join(launch["args"])});')
-  lines.append('  CHECK_ERR;')
+  if not launch.get('launched'):  # else `pre` launched the kernel itself
+    lines.append(f'  {kname}<<<grid, block, {smem}, stream>>>({", ".join(launch["args"])});')
+    lines.append('  CHECK_ERR;')
   lines.append('}')
   return '\n'.join(lines)
 

@@ -390,11 +390,11 @@ class _ColProg:
               f'    cudaEventRecord(lastEv[device], stream);',
               f'    lastStream[device] = stream;',
               f'    haveLast[device] = true;',
-              f'  }}',
-              f'  return;']
+              f'  }}']
     self.plan.smem_bytes = self.smem
     return {'kernel': kname, 'block': BT, 'elements_per_block': self.TE, 'smem': self.smem, 'args': args,
-            'grid': f'(numElements + {self.TE - 1}u) / {self.TE}u', 'pre': '\n'.join(pre)}
+            'grid': f'(numElements + {self.TE - 1}u) / {self.TE}u', 'pre': '\n'.join(pre),
+            'launched': bool(self.a_const_total)}
 
   # ------------------------------------------------------------------ pieces
   def _term(self, ti, t):

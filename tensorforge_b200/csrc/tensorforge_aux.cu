@@ -1,12 +1,14 @@
 // Implementation of include/tensorforge_aux.h (see there). Replaces
 // tensorforge/include/tensorforge_aux.cu:1-37.
 #include <cstdio>
+#include <string>
 #include <cuda_runtime.h>
 #include "tensorforge_aux.h"
 
 namespace {
 thread_local int tfb_last_status = 0;
-thread_local const char *tfb_prev_file = nullptr;
+// a copy: the caller's string is usually a temporary built from __FILE__
+thread_local std::string tfb_prev_file;
 thread_local int tfb_prev_line = 0;
 }  // namespace
 
@@ -19,11 +21,11 @@ void checkErr(const std::string &file, int line) {
 #ifndef NDEBUG
     std::fprintf(stderr, "\n%s, line %d: %s (%d)\n", file.c_str(), line, cudaGetErrorString(err),
                  static_cast<int>(err));
-    if (tfb_prev_line > 0) std::fprintf(stderr, "Previous CUDA call:\n%s, line %d\n", tfb_prev_file, tfb_prev_line);
+    if (tfb_prev_line > 0) std::fprintf(stderr, "Previous CUDA call:\n%s, line %d\n", tfb_prev_file.c_str(), tfb_prev_line);
 #endif
     return;
   }
-  tfb_prev_file = file.c_str();
+  tfb_prev_file = file;
   tfb_prev_line = line;
 }
 

@@ -136,6 +136,19 @@ class Generator:
     params.append(f'void* {GeneralLexicon.STREAM_PTR_STR}{" = nullptr" if with_defaults else ""}')
     return f'void launcher_{self._base_kernel_name}({", ".join(params)})'
 
+  def _status_entry(self):
+    """`extern "C" int tfb_launch_<name>(...)`: the launcher's parameters (no defaults),
+    returning the CUDA status of the launch (0 = success) for FFI callers that bind a
+    return code (ctypes, cgo). Emitted after the launcher; the launcher itself keeps the
+    reference's `void` signature and leaves the status for tensorforge_last_status()."""
+    proto = self._generate_launcher_proto(with_defaults=False)
+    args = [a.strip() for a in self._generate_base_params_list(with_types=False)]
+    args.append(GeneralLexicon.STREAM_PTR_STR)
+    return (f'\n\nextern "C" int tfb_launch_{self._base_kernel_name}{proto[proto.index("("):]} {{\n'
+            f'  (void)tensorforge_last_status();\n'
+            f'  launcher_{self._base_kernel_name}({", ".join(args)});\n'
+            f'  return tensorforge_last_status();\n}}')
+
   def abi_params(self):
     """[(c type, name)] of the launcher in order (used by the ctypes binding)."""
     out = []
@@ -190,6 +203,7 @@ class Generator:
     self._plan = make_plan(self._chain, self._context, self._tuned_variant())
     self._emitted = emit(self._chain, self._plan, self._context, self._base_kernel_name,
                          self._generate_launcher_proto(with_defaults=False), self._globals)
+    self._emitted.launcher += self._status_entry()
     self._kernel = self._emitted.kernel
     self._launcher = self._emitted.launcher
     self._header = f'extern "C" {self._generate_launcher_proto(with_defaults=True)};\n'

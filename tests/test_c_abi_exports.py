@@ -66,4 +66,5 @@ def test_generated_launcher_exports_reference_name():
   g = make('c0_gemm_ptr', 'float')
   lib = ctypes.CDLL(build_library(g.get_source()), mode=ctypes.RTLD_LOCAL)
   assert hasattr(lib, f'launcher_{g.get_base_name()}')
+  assert hasattr(lib, f'tfb_launch_{g.get_base_name()}')  # the status-returning form
   assert hasattr(lib, 'tensorforge_last_status')

@@ -35,7 +35,12 @@ def test_header_has_c_linkage_and_defaults():
   h = g.get_header()
   assert h.startswith('extern "C" void launcher_kernel_')
   assert 'unsigned* flags = nullptr, void* streamPtr = nullptr);' in h
-  assert g.get_launcher().count('launcher_') == 1
+  launcher = g.get_launcher()
+  assert launcher.count(f'extern "C" void launcher_{g.get_base_name()}(') == 1
+  # the status-returning entry point follows the launcher, same parameters without defaults
+  params = g._generate_launcher_proto(with_defaults=False).split('(', 1)[1]
+  assert f'extern "C" int tfb_launch_{g.get_base_name()}({params} {{' in launcher
+  assert 'nullptr' not in launcher.split('tfb_launch_')[1].split('{')[0]
 
 
 def test_call_sites():
