@@ -469,6 +469,7 @@ def impl_ours(args, rank, world, dist):
   variants = ['plain'] if args.variant == 'plain' else (
     [args.variant] if args.variant != 'auto' else ['tf32x3', 'fp16x3', 'plain', 'tf32x3_form_b', 'tf32x3_form_b2', 'tf32x3_form_b_ws'])
   opts_of = {'plain': {}, 'tf32x3': {'precision': 'tf32x3'}, 'fp16x3': {'precision': 'fp16x3'},
+             'tf32x3_ahead': {'precision': 'tf32x3', 'variant': {'form': 'u', 'ahead': 1}},
              'tf32x3_form_b': {'precision': 'tf32x3', 'variant': {'form': 'b'}},
              'tf32x3_form_b2': {'precision': 'tf32x3', 'variant': {'form': 'b', 'bbuf': 2}},
              'tf32x3_form_b_ws': {'precision': 'tf32x3', 'variant': {'form': 'b', 'ws': 1}},

@@ -156,7 +156,7 @@ def plan(chain, shape, precision, variant):
   # 4.8e8 for form U below
   if 'form' in variant:
     form = variant['form']
-  elif 'pipe' in variant or 'chunk' in variant:
+  elif 'pipe' in variant or 'chunk' in variant or 'ahead' in variant:
     form = 'u'
   else:
     form = 'b' if len(shape.terms) == 1 else 'u'
@@ -192,7 +192,10 @@ def plan(chain, shape, precision, variant):
   if smem > _plan.SMEM_LIMIT:
     return None
   chunk = variant.get('chunk', 16)
-  return Plan('tcsplit', {'precision': precision, 'chunk': chunk, 'pipe': pipe}, smem, 32 * (4 * H_GROUPS + 1),
+  params = {'precision': precision, 'chunk': chunk, 'pipe': pipe}
+  if int(variant.get('ahead', 0)) and pipe == 2:
+    params['ahead'] = 1
+  return Plan('tcsplit', params, smem, 32 * (4 * H_GROUPS + 1),
               note=f'M={shape.M} N={shape.N} terms={len(shape.terms)} tmem={lay["tmem_used"]} smem={sm["total"]}')
 
 
@@ -338,6 +341,7 @@ class _TC:
     self.pipe = plan_.params.get('pipe', 1)
     self.sm = smem_plan_v2(shape, self.prec) if self.pipe == 2 else smem_plan(shape, self.prec)
     self.LC = plan_.params['chunk']
+    self.ahead = bool(plan_.params.get('ahead', 0))
     self.H = H_GROUPS
     self.lines = []
     self.ind = 0
@@ -819,8 +823,11 @@ class _TC:
     self.w('const size_t el = e0 + le;')
     self.w('const bool active = lane_col && el < numElements && (flags == nullptr || flags[el] != 0u);')
     # per term: the MMA thread starts on a term as soon as its slot is full
-    for ti, t in enumerate(s.terms):
-      self._lane(ti, t, slot_base[ti], lim, f'(ubuf{ti} + row * {pitch}u)', True)
+    if self.ahead and self._ahead_ok():
+      self._lanes_ahead(slot_base, lim)
+    else:
+      for ti, t in enumerate(s.terms):
+        self._lane(ti, t, slot_base[ti], lim, f'(ubuf{ti} + row * {pitch}u)', True)
     self.close()
     self.w('if (!more) break;')
     self.w('prev_tile = tile; have_prev = true;')
@@ -890,6 +897,62 @@ class _TC:
     # buffer), and the stage / buffers are reused after the last term
     if self.sm['nbuf'] == 1 or ti == len(s.terms) - 1:
       self.w(f'tfb_tc::named_sync(1, {NP});')
+    self.close()
+
+  def _ahead_ok(self):
+    return (self.prec == 'tf32x3' and self.LC == 16 and
+            all(t.K % 4 == 0 and -(-self.lay['kpad'][ti] // 16) <= self.H for ti, t in enumerate(self.s.terms)))
+
+  def _lanes_ahead(self, slot_base, lim):
+    """Lane phases of all terms with the next term's column read and split while the
+    previous term's tensor-memory stores complete (plan option `ahead`). Two register sets
+    alternate; per thread the slot waits, stores and FULL arrivals keep the order of the
+    per-term lane phase."""
+    b, s = self.base, self.s
+    pitch = self.sm['pitch']
+    nterms = len(s.terms)
+    self.open('')
+    self.w('const unsigned c0 = grp * 16u;')
+    self.w('unsigned hv0[16], lv0[16], hv1[16], lv1[16];')
+
+    def load_split(ti, reg):
+      t = s.terms[ti]
+      self.open('')
+      self.w('float u[16];')
+      self.w('#pragma unroll')
+      self.w('for (int i = 0; i < 16; ++i) u[i] = 0.0f;')
+      self.open(f'if (active && c0 < {self.lay["kpad"][ti]}u)')
+      self.w(f'const float* p = (ubuf{ti} + row * {pitch}u) + c0;')
+      for v in range(4):
+        self.w(f'if (c0 + {4 * v}u < {t.K}u) {{ const float4 x = *reinterpret_cast<const float4*>(p + {4 * v}); '
+               f'u[{4*v}] = x.x; u[{4*v+1}] = x.y; u[{4*v+2}] = x.z; u[{4*v+3}] = x.w; }}')
+      self.close()
+      self.w('#pragma unroll')
+      self.w(f'for (int i = 0; i < 16; ++i) {{ hv{reg}[i] = tfb_tc::tf32_rna(u[i]); '
+             f'lv{reg}[i] = __float_as_uint(u[i] - __uint_as_float(hv{reg}[i])); }}')
+      self.close()
+
+    load_split(0, 0)
+    for ti in range(nterms):
+      reg = ti % 2
+      kp = self.lay['kpad'][ti]
+      acols = self.lay['a_cols'][ti]
+      slot_col = slot_base[ti]
+      self.w(f'if (it > 0 && !tfb_tc::mbar_wait(&bars[{nterms + ti}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, {30 + ti}u); }}')
+      self.w('tfb_tc::fence_after();')
+      self.open(f'if (c0 < {kp}u)')
+      self.w(f'tfb_tc::st_x8(lane_addr + {slot_col}u + c0, hv{reg});')
+      self.w(f'tfb_tc::st_x8(lane_addr + {slot_col + acols}u + c0, lv{reg});')
+      self.open(f'if (c0 + 8u < {kp}u)')
+      self.w(f'tfb_tc::st_x8(lane_addr + {slot_col + 8}u + c0, hv{reg} + 8);')
+      self.w(f'tfb_tc::st_x8(lane_addr + {slot_col + acols + 8}u + c0, lv{reg} + 8);')
+      self.close()
+      self.close()
+      if ti + 1 < nterms:
+        load_split(ti + 1, (ti + 1) % 2)
+      self.w('tfb_tc::st_wait();')
+      self.w('tfb_tc::fence_before();')
+      self.w(f'tfb_tc::mbar_arrive(&bars[{ti}]);')
     self.close()
 
   def _lane(self, ti, t, slot_col, lim, src, vec):

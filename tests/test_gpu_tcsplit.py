@@ -168,3 +168,25 @@ def test_form_b_flags_and_loguniform(form):
     assert np.array_equal(got[s:s + 504], ref[s:s + 504])
   got, ref, _, _ = _run('chain_o6', 'tf32x3', 777, dist='loguniform', variant=dict(form))
   assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-6
+
+
+FORM_U_AHEAD = {'form': 'u', 'ahead': 1}
+
+
+@pytest.mark.parametrize('n', [1, 13, 14, 15, 333, 4099])
+def test_form_u_split_ahead(n):
+  """Form U with the next term's column read and split while the previous term's tensor
+  memory stores complete (plan option `ahead`): sizes around the 14-element tile, flags,
+  log-uniform values."""
+  from tensorforge_b200.kernels import make
+  assert make('chain_o6', 'float', precision='tf32x3', variant=dict(FORM_U_AHEAD)).get_plan().params.get('ahead') == 1
+  got, ref, _, _ = _run('chain_o6', 'tf32x3', n, variant=dict(FORM_U_AHEAD))
+  assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-6
+  if n == 333:
+    got, ref, out, flags = _run('chain_o6', 'tf32x3', 611, use_flags=True, variant=dict(FORM_U_AHEAD))
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-6
+    for e in np.nonzero(flags == 0)[0][:5]:
+      s = out.starts[e]
+      assert np.array_equal(got[s:s + 504], ref[s:s + 504])
+    got, ref, _, _ = _run('chain_o6', 'tf32x3', 777, dist='loguniform', variant=dict(FORM_U_AHEAD))
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-6
