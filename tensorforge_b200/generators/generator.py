@@ -233,6 +233,13 @@ class Generator:
   def get_header(self):
     return self._header
 
+  def get_status_header(self):
+    """Declaration of the status-returning twin of the launcher (`tfb_launch_<name>`,
+    emitted after the launcher by `get_launcher()`); `get_header()` stays the reference's
+    single prototype."""
+    proto = self._generate_launcher_proto(with_defaults=True)
+    return f'extern "C" int tfb_launch_{self._base_kernel_name}{proto[proto.index("("):]};\n'
+
   # ------------------------------------------------------------------ additions
   def get_source(self):
     """A complete .cu translation unit (includes + kernel + launcher)."""

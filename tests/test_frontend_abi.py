@@ -41,6 +41,7 @@ def test_header_has_c_linkage_and_defaults():
   params = g._generate_launcher_proto(with_defaults=False).split('(', 1)[1]
   assert f'extern "C" int tfb_launch_{g.get_base_name()}({params} {{' in launcher
   assert 'nullptr' not in launcher.split('tfb_launch_')[1].split('{')[0]
+  assert g.get_status_header() == h.replace('extern "C" void launcher_', 'extern "C" int tfb_launch_')
 
 
 def test_call_sites():
