@@ -133,6 +133,19 @@ EW_BENCH_VARIANTS = [
 ]
 
 
+def mixed_catalogue():
+  """(name, Generator) for the groups of the mixed-shape workload under their own default
+  plans (the benchmark's separate-launch comparison and the large-basis parity tests)."""
+  from . import workloads as cases
+  ns = cases.ns_from_module('tensorforge_b200')
+  out = []
+  for b, q, _ in cases.mixed_shape_groups():
+    g = Generator(cases.mixed_chain(ns, b, q), Context('sm_100a', 'cuda', FP['float']))
+    g.generate()
+    out.append((f'mixed_{b}x{q}', g))
+  return out
+
+
 def grouped_catalogue():
   """Grouped (mixed-shape) kernels used by the tests and the benchmark."""
   from . import workloads as cases

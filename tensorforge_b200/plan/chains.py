@@ -179,9 +179,15 @@ def r_slots(term):
 
 
 # Column programs unroll one FMA per nonzero of every A_t into straight-line code. Above
-# this many the instruction stream outgrows the SM's instruction caches and ptxas time grows
-# to minutes per kernel, so such chains go to the generic generator.
-COLPROG_MAX_FMAS = 6144
+# this many ptxas time grows past a minute per kernel, so such chains go to the generic
+# generator. Measured on B200 (84x84 A at 45 %, three terms, 9,533 FMAs per column, 26 s of
+# ptxas, 226 registers, no spills): 2.13e7 against 2.30e6 el/s for the generic kernel with 27
+# quantities and 8.25e7 against 1.04e7 with 9, so the larger code still pays many times over.
+COLPROG_MAX_FMAS = 16384
+# A 128-thread column program whose shared memory leaves room for only one CTA per SM runs
+# with 256 threads instead when that keeps the prefetch stage (same registers per thread,
+# twice the warps per SM; 2.0x and 1.9x faster on the two 84-basis chains above).
+COLPROG_SMEM_PER_SM = 228 * 1024
 # A values as constant-bank FMA operands stay in the immediate-constant cache up to roughly
 # this many values. Measured on B200: constant A is fastest for most random chains with at
 # most 2,048 values and for the dense 56x56 GEMM (3,136 values: 2.54e8 vs 2.32e8 el/s);
@@ -198,8 +204,19 @@ COLPROG_CONST_MIXED = 2048
 
 
 def colprog_plan(chain, shape: LeftChain, fp_size, variant):
+  if 'threads' in variant:
+    return _colprog_plan(chain, shape, fp_size, variant, variant['threads'])
+  p = _colprog_plan(chain, shape, fp_size, variant, 128)
+  if p is not None and 2 * (p.smem_bytes + 1024) > COLPROG_SMEM_PER_SM:
+    wide = _colprog_plan(chain, shape, fp_size, variant, 256)
+    # only where the wider tile keeps the prefetch stage (measured only in that form)
+    if wide is not None and wide.params['prefetch'] >= p.params['prefetch']:
+      return wide
+  return p
+
+
+def _colprog_plan(chain, shape: LeftChain, fp_size, variant, threads):
   from ..codegen.colprog import tile_elements
-  threads = variant.get('threads', 128)
   chunk = variant.get('chunk', 16)
   sizes = [t.A.storage_size() for t in shape.terms]
   a_total = sum(sizes)
@@ -223,7 +240,7 @@ def colprog_plan(chain, shape: LeftChain, fp_size, variant):
   chunk = max(vec, (chunk + vec - 1) // vec * vec)
   if shape.M > 128 or shape.N > threads:
     return None
-  if a_total > COLPROG_MAX_FMAS:
+  if a_total > COLPROG_MAX_FMAS and variant.get('strategy') != 'colprog':
     return None
   cols = int(variant.get('cols', 1))
   te = tile_elements(shape, threads, cols)

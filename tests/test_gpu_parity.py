@@ -116,3 +116,38 @@ def test_column_program_variants_match_reference(case, variant):
     ref = z[f'out_{s["name"]}'].astype(np.float64)
     scale = max(1e-30, float(np.abs(ref).max()))
     assert np.abs(out[s['name']] - ref).max() <= 1e-5 * scale, s['name']
+
+
+@pytest.mark.parametrize('n', [1, 9, 10, 28, 1001])
+@pytest.mark.parametrize('quantities', [9, 27])
+def test_large_basis_column_program(quantities, n):
+  """84-basis chains (9.5k unrolled FMAs per column, 256-thread CTAs by default) against the
+  FP64 oracle, at sizes around the tile (9 elements for 27 quantities, 28 for 9), with flags."""
+  import torch
+  from oracle import harness, multilinear
+  from tensorforge_b200.kernels import mixed_catalogue
+  from tensorforge_b200.runtime import compile_generator
+  g = dict(mixed_catalogue())[f'mixed_84x{quantities}']
+  assert g.get_plan().strategy == 'colprog' and g.get_plan().params['threads'] == 256
+  k = compile_generator(g)
+  descrs = g.descr_list
+  lay, mem = harness.make_memory(descrs, n, seed=5)
+  flags = harness.make_flags(n, 5)
+  dev = {l.name: torch.tensor(mem.buffers[l.name], dtype=torch.float32, device='cuda') for l in lay if l.kind != 'scalar'}
+  kw = {'numElements': n, 'flags': torch.tensor(flags, dtype=torch.int32, device='cuda')}
+  for l in lay:
+    kw[l.name] = dev[l.name]
+    if l.kind == 'strided':
+      kw[f'{l.name}_extraOffset'] = l.extra_offset
+  assert all(l.kind in ('strided', 'shared') for l in lay)
+  k(**kw)
+  torch.cuda.synchronize()
+  multilinear.evaluate(descrs, mem, n, flags=flags)
+  for l in lay:
+    if l.kind == 'strided' and l.tensor.direction.name != 'SOURCE':
+      got = dev[l.name].double().cpu().numpy()
+      ref = mem.buffers[l.name]
+      assert np.linalg.norm(got - ref) <= 1e-6 * np.linalg.norm(ref)
+      for e in np.nonzero(flags == 0)[0]:  # masked elements keep their values exactly
+        s = l.starts[e]
+        assert np.array_equal(got[s:s + 84 * quantities], ref[s:s + 84 * quantities])
