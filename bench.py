@@ -354,6 +354,11 @@ def extra_workloads(stream, short=False):
       k(**kw)
   total2, per2 = time_launches(separate, stream, 5, 2)
   ms2 = sum(per2) / len(per2)
+  # the same batch as one CUDA graph of per-group kernels on 4 side streams
+  pg = gk.prepare_per_group(kws, streams=4)
+  pg.capture()
+  _, per3 = time_launches(pg.replay, stream, 10, 3)
+  ms3 = sum(per3) / len(per3)
   per_group = []
   for i, (b, q, n) in enumerate(groups):  # the same launch with every other group emptied
     one = gk.prepare([dict(kw, numElements=(kw['numElements'] if j == i else 0)) for j, kw in enumerate(kws)])
@@ -365,6 +370,8 @@ def extra_workloads(stream, short=False):
   out['c3_mixed_shapes'] = {'elements': total_el, 'groups': len(groups), 'elements_per_s': total_el / (ms / 1e3),
                             'nz_gflops': nz / (ms / 1e3) / 1e9, 'ms': ms, 'launch': 'one persistent kernel, CUDA graph replay',
                             'separate_launches_ms': ms2, 'separate_elements_per_s': total_el / (ms2 / 1e3),
+                            'graph_per_group_ms': ms3, 'graph_per_group_elements_per_s': total_el / (ms3 / 1e3),
+                            'graph_per_group': 'one CUDA graph: each group through its own launcher, 4 side streams',
                             'per_group': per_group}
   # config 2: log-uniform magnitudes through every precision variant, error vs the FP64 oracle
   descrs = cases.build(CASE, cases.ns_from_module('tensorforge_b200'))

@@ -313,6 +313,76 @@ class GroupedKernel:
     counter = torch.zeros(1, dtype=torch.int32, device='cuda')
     return GroupedLaunch(self, dev_args, dev_items, len(items), counter, keep)
 
+  def prepare_per_group(self, group_kwargs, streams=4):
+    """The same argument sets as `prepare`, launched group by group through each
+    generator's own launcher on `streams` side streams. Returns a `PerGroupLaunch`."""
+    from .runtime import compile_generator
+    if len(group_kwargs) != len(self.gens):
+      raise ValueError('one argument set per group is required')
+    return PerGroupLaunch([compile_generator(g) for g in self.gens], group_kwargs, streams)
+
+
+class PerGroupLaunch:
+  """The same mixed-shape batch with every group through its own launcher (the planner's
+  own plan for its shape: prefetch stage, CTA width, constant or shared A), the groups spread
+  over side streams (largest work first, onto the least-loaded stream) and joined back on the
+  caller's stream; `capture()` records fork, launches and join in one CUDA graph.
+
+  Against the persistent kernel it gives up the single launch and the shared work table (all
+  groups there run one CTA shape, without the prefetch stage) for per-shape kernels.
+  """
+
+  def __init__(self, kernels, group_kwargs, streams):
+    self.kernels = kernels
+    self.kwargs = [dict(kw) for kw in group_kwargs]
+    work = [int(kw['numElements']) * k.generator.get_chain().nz_flops_per_element()
+            for k, kw in zip(kernels, group_kwargs)]
+    load = [0] * max(1, streams)
+    self.lanes = [[] for _ in load]
+    for gid in sorted(range(len(kernels)), key=lambda i: -work[i]):
+      lane = min(range(len(load)), key=lambda i: load[i])
+      self.lanes[lane].append(gid)
+      load[lane] += work[gid]
+    self.streams = None
+    self.graph = None
+
+  def launch(self, stream=None):
+    import torch
+    st = stream if stream is not None else torch.cuda.current_stream()
+    if self.streams is None:
+      self.streams = [torch.cuda.Stream() for _ in self.lanes]
+    used = []
+    for side, gids in zip(self.streams, self.lanes):
+      gids = [g for g in gids if int(self.kwargs[g]['numElements']) > 0]
+      if not gids:
+        continue
+      side.wait_stream(st)
+      for gid in gids:
+        self.kernels[gid](**dict(self.kwargs[gid], streamPtr=side.cuda_stream))
+      used.append(side)
+    for side in used:
+      st.wait_stream(side)
+
+  def capture(self):
+    """Record the launch in a CUDA graph (after one eager launch for first-call setup)."""
+    import torch
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+      self.launch(s)
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+      self.launch(torch.cuda.current_stream())
+    self.graph = g
+    return g
+
+  def replay(self):
+    if self.graph is None:
+      self.capture()
+    self.graph.replay()
+
 
 def host_records(kernel, group_kwargs):
   """tfb_group_args records in host memory (for the allocation-free entry point)."""
