@@ -9,7 +9,7 @@ generated kernel over all elements. The chain is generated through the public fr
 (`Generator`) and called through the emitted C-ABI launcher.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--variant auto|plain|tf32x3|fp16x3|bf16x3] [--elements E]
+                  [--variant auto|plain|tf32x3|bf16x3|tf32x3_form_b|...] [--elements E]
                   [--workload chain_o6|ew_update]
 
 `--workload ew_update` measures the elementwise stage alone instead (its own JSON line).
@@ -474,8 +474,8 @@ def impl_ours(args, rank, world, dist):
   device = torch.device('cuda', torch.cuda.current_device())
   n = args.elements
   variants = ['plain'] if args.variant == 'plain' else (
-    [args.variant] if args.variant != 'auto' else ['tf32x3', 'fp16x3', 'plain', 'tf32x3_form_b', 'tf32x3_form_b2', 'tf32x3_form_b_ws'])
-  opts_of = {'plain': {}, 'tf32x3': {'precision': 'tf32x3'}, 'fp16x3': {'precision': 'fp16x3'},
+    [args.variant] if args.variant != 'auto' else ['tf32x3', 'plain', 'tf32x3_form_b', 'tf32x3_form_b2', 'tf32x3_form_b_ws'])
+  opts_of = {'plain': {}, 'tf32x3': {'precision': 'tf32x3'},
              'tf32x3_ahead': {'precision': 'tf32x3', 'variant': {'form': 'u', 'ahead': 1}},
              'tf32x3_form_b': {'precision': 'tf32x3', 'variant': {'form': 'b'}},
              'tf32x3_form_b2': {'precision': 'tf32x3', 'variant': {'form': 'b', 'bbuf': 2}},

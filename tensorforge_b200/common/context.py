@@ -10,7 +10,7 @@ from .basic_types import FloatingPointType
 
 SUPPORTED_ARCHS = ('sm_100', 'sm_100a')
 SUPPORTED_BACKENDS = ('cuda',)
-PRECISIONS = ('plain', 'tf32x3', 'bf16x3', 'fp16x3', 'dmma', 'auto')
+PRECISIONS = ('plain', 'tf32x3', 'bf16x3', 'dmma')
 TUNERS = ('heuristic', 'exhaustive', 'model')
 
 

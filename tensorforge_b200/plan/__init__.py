@@ -74,7 +74,7 @@ def make_plan(chain, context, variant=None):
   if forced in (None, 'colprog', 'tcsplit'):
     shape = chainplan.match_left_chain(chain)
     if shape is not None:
-      if precision in ('tf32x3', 'bf16x3', 'fp16x3') and context.fp_type == FloatingPointType.FLOAT and forced != 'colprog':
+      if precision in ('tf32x3', 'bf16x3') and context.fp_type == FloatingPointType.FLOAT and forced != 'colprog':
         p = chainplan.tcsplit_plan(chain, shape, precision, variant)
         if p is not None:
           return p

@@ -28,3 +28,10 @@ def test_two_cta_column_programs_stay_at_128_threads():
   # the FP64 column program would lose its prefetch stage at 256 threads: not widened
   p = make('chain_o6', 'double', variant={'strategy': 'colprog'}).get_plan()
   assert p.params['threads'] == 128 and p.params['prefetch'] == 1
+
+
+def test_unimplemented_precisions_are_rejected():
+  import pytest
+  for p in ('fp16x3', 'auto', 'fp8'):
+    with pytest.raises(ValueError):
+      Options(precision=p)
