@@ -10,9 +10,10 @@ generated kernel over all elements. The chain is generated through the public fr
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--variant auto|plain|tf32x3|bf16x3|tf32x3_form_b|...] [--elements E]
-                  [--workload chain_o6|ew_update]
+                  [--workload chain_o6|ew_update|mixed] [--basis B --quantities Q]
 
-`--workload ew_update` measures the elementwise stage alone instead (its own JSON line).
+`--workload ew_update` measures the elementwise stage alone instead (its own JSON line);
+`--workload mixed` one group of the mixed-shape workload (84 x 27 by default).
 
 For N > 1 the driver launches one process per GPU (torchrun); elements are independent, so
 each rank runs its own 500,000 elements (weak scaling) with no collective on the data
@@ -675,6 +676,49 @@ def impl_elementwise(args):
     'gpu_launches': args.steps, 'clocks': clocks.summary()}))
 
 
+def impl_mixed_group(args):
+  """`--workload mixed`: one group of the mixed-shape workload alone (basis x quantities,
+  three sparse basis x basis K terms at 45 %, a sparse quantity x quantity S per element and
+  term) under its default plan, device-resident inputs; FP32 roofline on the nz flops with
+  the FMA probe of the same run; error of the first 256 elements against the FP64 oracle."""
+  import torch
+  from tensorforge_b200 import workloads as cases
+  from tensorforge_b200.common.basic_types import FloatingPointType
+  from tensorforge_b200.common.context import Context
+  from tensorforge_b200.generators.generator import Generator
+  from tensorforge_b200.runtime import compile_generator
+  torch.cuda.set_device(0)
+  ns = cases.ns_from_module('tensorforge_b200')
+  n, b, q = args.elements, args.basis, args.quantities
+  g = Generator(cases.mixed_chain(ns, b, q), Context('sm_100a', 'cuda', FloatingPointType.FLOAT))
+  g.generate()
+  k = compile_generator(g)
+  bufs = make_inputs(g, n, torch.device('cuda'), seed=1)
+  kw = {t.name: bufs[t.name] for t, _ in g.abi_symbols()}
+  kw['numElements'] = n
+  k(**kw)
+  torch.cuda.synchronize()
+  acc = check_accuracy(cases.mixed_chain(ns, b, q), g, bufs, min(n, 256))
+  stream = torch.cuda.current_stream()
+  with Clocks(index=torch.cuda.current_device()) as clocks:
+    total, per = time_launches(lambda: k(**kw), stream, args.steps, max(3, args.warmup))
+  launch = sum(per) / len(per)
+  nz = g.get_chain().nz_flops_per_element()
+  peak = fp32_peak_cached()
+  flops = n * nz / (launch / 1e3)
+  print(json.dumps({
+    'metric': 'mixed-shape group elements/s', 'value': n / (total / args.steps / 1e3), 'unit': 'elements/s',
+    'n_gpus': 1, 'steps': args.steps, 'warmup': max(3, args.warmup), 'ms_per_step': total / args.steps,
+    'higher_is_better': True, 'dtype': 'f32', 'data': 'synthetic',
+    'config': {'workload': f'mixed-shape group: {b} basis functions, {q} quantities, FP32', 'elements': n,
+               'plan': g.get_plan().key()},
+    'accuracy': acc,
+    'roofline': {'bound': 'fp32', 'achieved': flops / 1e12, 'peak': peak / 1e12, 'unit': 'TFLOP/s',
+                 'frac': flops / peak, 'flops_per_element': nz, 'kernel': g.get_base_name(),
+                 'peak_source': 'measured FP32 FFMA probe (libtfb200_runtime tfb_fma_peak_launch), same run'},
+    'gpu_launches': args.steps, 'clocks': clocks.summary()}))
+
+
 def main():
   ap = argparse.ArgumentParser()
   ap.add_argument('--gpus', type=int, default=1)
@@ -686,11 +730,17 @@ def main():
   ap.add_argument('--ref-sample', type=int, default=4096)
   ap.add_argument('--no-cpu', action='store_true')
   ap.add_argument('--no-extras', action='store_true')
-  ap.add_argument('--workload', default='chain_o6', choices=['chain_o6', 'ew_update'],
-                  help='chain_o6: the headline order-6 chain; ew_update: the elementwise stage alone')
+  ap.add_argument('--workload', default='chain_o6', choices=['chain_o6', 'ew_update', 'mixed'],
+                  help='chain_o6: the headline order-6 chain; ew_update: the elementwise stage alone; '
+                       'mixed: one group of the mixed-shape workload (--basis, --quantities)')
+  ap.add_argument('--basis', type=int, default=84)
+  ap.add_argument('--quantities', type=int, default=27)
   args = ap.parse_args()
   if args.workload == 'ew_update':
     impl_elementwise(args)
+    return
+  if args.workload == 'mixed':
+    impl_mixed_group(args)
     return
   from tensorforge_b200.runtime import ranks
   rank, world, _ = ranks.env_rank()
