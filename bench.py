@@ -32,6 +32,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = 'order-6 chain elements/s: split-TC vs plain FP32, same B200, rel err≤1e-6'
 CASE = 'chain_o6'
+WORKLOAD = 'order-6 volume chain: out(56x9) = sum_3 K(56x56, 45% sparse) Q(56x9) S(9x9, 24 nnz), FP32'
 FALLBACK_HBM = 6650.0
 
 
@@ -261,7 +262,7 @@ def impl_reference(args, rank, world):
     'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': 'elements/s', 'n_gpus': world,
     'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True,
     'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
-    'config': {'workload': 'order-6 volume chain 56x9, 3 terms, K 45% sparse, S 24 nnz, FP32',
+    'config': {'workload': WORKLOAD,
                'elements_per_step': n, 'full_workload_elements': args.elements},
     'cpu_baseline': {'value': value, 'unit': 'elements/s', 'cores': r['cores'], 'kind': 'reference',
                      'sample': f'{n} elements per step (bounded sample of the {args.elements}-element workload), '
@@ -603,7 +604,7 @@ def impl_ours(args, rank, world, dist):
     'metric': METRIC, 'value': value, 'unit': 'elements/s', 'n_gpus': world, 'steps': args.steps,
     'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
     'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
-    'config': {'workload': 'order-6 volume chain: out(56x9) = sum_3 K(56x56, 45% sparse) Q(56x9) S(9x9, 24 nnz), FP32',
+    'config': {'workload': WORKLOAD,
                'elements_per_gpu': n, 'variant': primary, 'plan': pr['plan'],
                'l2': 'inputs larger than L2 (no flush)'},
     'accuracy': pr['accuracy'],
