@@ -219,7 +219,7 @@ def _cpu_bench(args_list):
   """Run oracle/cpu_bench.py in a fresh interpreter (system OpenMP runtime) and parse its JSON."""
   cmd = [sys.executable, '-m', 'oracle.cpu_bench'] + args_list
   env = dict(os.environ)
-  env.setdefault('OMP_TARGET_OFFLOAD', 'DISABLED')
+  env['OMP_TARGET_OFFLOAD'] = 'DISABLED'  # the CPU baseline never runs on an offload device
   proc = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, env=env, timeout=900)
   if proc.returncode != 0:
     log(proc.stderr[-2000:])

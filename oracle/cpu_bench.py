@@ -28,7 +28,7 @@ def main():
   ap.add_argument('--steps', type=int, default=1)
   ap.add_argument('--warmup', type=int, default=1)
   a = ap.parse_args()
-  os.environ.setdefault('OMP_TARGET_OFFLOAD', 'DISABLED')
+  os.environ['OMP_TARGET_OFFLOAD'] = 'DISABLED'  # the CPU baseline never runs on an offload device
   import numpy as np
   from oracle import cases, harness, ref_omp
   rk = ref_omp.RefKernel(a.tag)
