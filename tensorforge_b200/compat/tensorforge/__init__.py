@@ -13,6 +13,7 @@ lexics, the hardware database) have no counterpart: the sm_100a generators repla
 """
 import importlib
 import sys
+import types
 
 _MODULES = [
   'common', 'common.aux', 'common.basic_types', 'common.context', 'common.exceptions', 'common.operation',
@@ -25,8 +26,11 @@ for _name in _MODULES:
   sys.modules[f'{__name__}.{_name}'] = importlib.import_module(f'tensorforge_b200.{_name}')
 # the reference keeps the architecture description in common/vm/vm.py; here it is part of
 # common/context.py (VM, vm_factory)
-for _name in ('common.vm', 'common.vm.vm'):
-  sys.modules[f'{__name__}.{_name}'] = sys.modules['tensorforge_b200.common.context']
+_vm_pkg = types.ModuleType(f'{__name__}.common.vm')
+_vm_pkg.__path__ = []
+_vm_pkg.vm = sys.modules['tensorforge_b200.common.context']
+sys.modules[f'{__name__}.common.vm'] = _vm_pkg
+sys.modules[f'{__name__}.common.vm.vm'] = _vm_pkg.vm
 for _name in ('common', 'generators', 'frontend'):
   setattr(sys.modules[__name__], _name, sys.modules[f'{__name__}.{_name}'])
 

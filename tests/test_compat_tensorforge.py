@@ -49,6 +49,7 @@ def test_reference_example_imports_resolve():
     'from tensorforge.generators.descriptions import GemmDescr, MultilinearDescr, FloatingPointType, Addressing',
     'from tensorforge.generators.generator import Generator',
     'from tensorforge.common.vm.vm import vm_factory',
+    'from tensorforge.common.vm import vm; assert vm.vm_factory is vm_factory',
     'from tensorforge.generators.optree import Assignment',
     'from tensorforge import get_routine_generator, get_cmake_path, print_cmake_path, use_fusedgemm_cost',
     'import tensorforge.functions as f; f.tensor; f.scalar; f.assign',
