@@ -55,7 +55,8 @@ class Clocks:
   def __init__(self, index=0):
     self.index = index
     self.proc = None
-    self.path = os.path.join(ROOT, 'gpurun_out', f'clocks_{os.getpid()}.csv')
+    import tempfile
+    self.path = os.path.join(tempfile.gettempdir(), f'tfb_clocks_{os.getpid()}_{index}.csv')
 
   def __enter__(self):
     os.makedirs(os.path.dirname(self.path), exist_ok=True)
@@ -78,8 +79,16 @@ class Clocks:
       self.proc.terminate()
       self.proc.wait()
       self.f.close()
+      self._summary = self._read()
+      try:
+        os.remove(self.path)
+      except OSError:
+        pass
 
   def summary(self):
+    return getattr(self, '_summary', None)
+
+  def _read(self):
     if self.proc is None or not os.path.exists(self.path):
       return None
     mhz, mx, reasons = [], 0, set()

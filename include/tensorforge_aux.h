@@ -2,8 +2,8 @@
 //
 // Replaces tensorforge/include/tensorforge_aux.h:1-15 (CHECK_ERR, tensorforge::checkErr,
 // tensorforge::synchDevice) with the same names and meaning, for the CUDA backend on
-// B200. Differences: checkErr never throws (a launcher with C linkage must not unwind);
-// it records the CUDA error as a status code, readable and clearable through
+// B200. Differences: checkErr never throws (each launcher is also called from its C-linkage
+// twin tfb_launch_<name>, which must not unwind into C or ctypes callers); it records the CUDA error as a status code, readable and clearable through
 // tensorforge_last_status(), and prints it unless NDEBUG is defined.
 #ifndef TENSORFORGE_INTERNALS_H
 #define TENSORFORGE_INTERNALS_H

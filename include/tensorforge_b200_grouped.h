@@ -25,8 +25,12 @@ struct tfb_group_args {
 };
 #endif
 
-// Largest number of groups the allocation-free entry point accepts.
+// Largest number of groups the allocation-free entry point accepts (its group records
+// travel as one kernel parameter: 64 records are 13 KB of the 32 KB parameter space).
 #define TFB_NOALLOC_MAX_GROUPS 64
+// Size, in 32-bit words, of the allocation-free entry point's static device scratch (the
+// work counter; one word used).
+#define TFB_NOALLOC_SCRATCH_WORDS 64
 
 #ifdef __cplusplus
 #define TFB_EXTERN_C extern "C"
@@ -42,12 +46,16 @@ struct tfb_group_args {
                                             unsigned num_items, unsigned* counter,          \
                                             void* stream);                                  \
   /* Allocation-free form (no counterpart in the reference): for callers that cannot call   \
-     cudaMalloc. host_args: num_groups tfb_group_args records in host memory (at most        \
-     TFB_NOALLOC_MAX_GROUPS and the size of the fused set). The scratch lives in a static   \
-     device array of the library (work counter, tile offsets, records: ~13 KB per GPU, kept \
-     until exit); the first call on a device resolves its address (call it once before any  \
-     stream capture). Calls that overlap on the GPU share that scratch and race.            \
-     Returns a cudaError_t value, cudaErrorInvalidValue for too many groups. */             \
+     cudaMalloc (code under an external memory manager that owns every device allocation,  \
+     latency-critical loops where an allocation could block). host_args: num_groups         \
+     tfb_group_args records in host memory (at most TFB_NOALLOC_MAX_GROUPS and the size of  \
+     the fused set), passed to the kernel by value: reusable once the call returns. The     \
+     work counter lives in a static device array of the library (256 bytes per GPU, kept    \
+     until exit), cleared on `stream` by every call. The first call on a device looks up    \
+     its address (make that call before any stream capture; the address is not refreshed   \
+     after cudaDeviceReset). Calls that overlap on the GPU share the counter and race.      \
+     Returns a cudaError_t value, cudaErrorInvalidValue for a null host_args or too many    \
+     groups. */                                                                              \
   TFB_EXTERN_C int tfb_grouped_launch_noalloc_##set(const void* host_args,                  \
                                                     unsigned num_groups, void* stream);
 

@@ -10,7 +10,7 @@ reference's `tensorforge/include/tensorforge_aux_target.cpp` using
 The compiled libraries are then loaded with ctypes (this part needs no source tree, so
 it also runs on a machine that only received the built files).
 
-Caveats from the reference (SURVEY-level facts restated): the emitted region is `nowait`,
+Caveats from the reference: the emitted region is `nowait`,
 so the entry point ends with `#pragma omp taskwait`; element counts must be a multiple
 of the kernel's elements-per-block, because the emitted barrier sits inside the
 element guard (target_lexic.py:147-168, generator.py:145-146) - callers pad N and mask
@@ -26,7 +26,16 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_OUT = os.path.join(HERE, '_ref')
-REFERENCE_ROOT = os.environ.get('TFB_REFERENCE_ROOT', '/root/reference')
+# The read-only reference checkout this recipe reads (generator sources and
+# tensorforge/include). Set TFB_REFERENCE_ROOT to use another checkout; every other
+# script that needs the reference tree takes the path from here.
+DEFAULT_REFERENCE_ROOT = '/root/reference'
+REFERENCE_ROOT = os.environ.get('TFB_REFERENCE_ROOT', DEFAULT_REFERENCE_ROOT)
+
+
+def reference_present():
+  """True when the reference generator sources are readable at REFERENCE_ROOT."""
+  return os.path.isdir(os.path.join(REFERENCE_ROOT, 'tensorforge'))
 
 
 def _reference_ns():

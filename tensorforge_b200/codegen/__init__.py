@@ -1,8 +1,10 @@
 """sm_100a code generators and the launcher emitter.
 
-`emit` turns a planned chain into the kernel text and a launcher whose name and
-parameter list are the reference CUDA backend's (tensorforge/generators/generator.py:
-164-196, :426-436), with C linkage so it can be bound from C, C++, ctypes or torch.
+`emit` turns a planned chain into the kernel text and a launcher whose name, parameter
+list and C++ linkage are the reference CUDA backend's (tensorforge/generators/generator.py:
+164-196, :426-436), so object code compiled against the reference's declaration links
+unchanged. C, ctypes and other FFI callers bind `tfb_launch_<name>` instead (emitted by
+the generator after the launcher, `extern "C"`, same parameters, returning the status).
 Launcher behaviour kept from the reference: `streamPtr` is a `cudaStream_t` (nullptr ->
 default stream), the launch is asynchronous, the caller owns every buffer and pointer
 array and the launcher allocates nothing, and errors go through `CHECK_ERR`.
@@ -41,7 +43,7 @@ def emit_launcher(proto, launch):
   smem = launch['smem']
   grid_expr = launch.get('grid', f'(numElements + {epb} - 1) / {epb}')
   pre = launch.get('pre', '')
-  lines = [f'extern "C" {proto} {{']
+  lines = [f'{proto} {{']
   lines.append('  if (numElements == 0) return;')
   lines.append(f'  const size_t blocks = {grid_expr};')
   lines.append(f'  dim3 block({launch["block"]}, 1, 1);')

@@ -206,7 +206,7 @@ class Generator:
     self._emitted.launcher += self._status_entry()
     self._kernel = self._emitted.kernel
     self._launcher = self._emitted.launcher
-    self._header = f'extern "C" {self._generate_launcher_proto(with_defaults=True)};\n'
+    self._header = f'{self._generate_launcher_proto(with_defaults=True)};\n'
 
   def _tuned_variant(self):
     """Variant picked by Options.tuner ('model' / 'exhaustive'), None for the planner's own.

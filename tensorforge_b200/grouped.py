@@ -141,42 +141,49 @@ class GroupedKernel:
   def _noalloc_variant(self, work_vals):
     """An entry point for callers that cannot allocate device memory.
 
-    Some callers cannot call cudaMalloc: code running where the device allocator is off
-    limits (inside a host callback, under an external memory manager that owns every
-    allocation, or in a tight real-time loop where an allocation could block). For them
-    this variant keeps its scratch - the work counter, the per-group tile offsets and the
-    group argument records - in a file-scope device array of fixed size instead of
-    caller-provided buffers; the caller still passes every input and output.
+    Some callers cannot call cudaMalloc: code running under an external memory manager
+    that owns every device allocation (a host application that hands this library
+    pre-sized buffers only), or a latency-critical loop where an allocation could block
+    on a device-wide synchronisation. The regular entry point needs two device buffers
+    besides the operands (the work table and the work counter); this variant needs
+    neither. The group records and per-group tile offsets travel by value as one kernel
+    parameter (`__grid_constant__`, so no host buffer is referenced once the call
+    returns), and the one piece of device scratch, the work counter, sits in a file-scope
+    device array of the library. The caller still passes every input and output.
     """
     T, BT, G = self.T, self.threads, len(self.gens)
     te = ', '.join(str(t) for t in self.te)
+    n = self.name
     k = ['',
-         '// Scratch of the allocation-free entry point: every GPU that loads this library keeps',
-         '// one copy until the process exits. All calls share it and it keeps the last call\'s',
-         '// contents, so calls that overlap on the GPU (different streams, no ordering) race.',
-         'struct tfb_noalloc_scratch {',
-         '  unsigned counter;',
-         '  unsigned num_groups;',
-         '  unsigned tile_prefix[TFB_NOALLOC_MAX_GROUPS + 1];',
-         '  tfb_group_args args[TFB_NOALLOC_MAX_GROUPS];',
-         '};',
-         'static __device__ __align__(256) unsigned char tfb_noalloc_scratch_storage[sizeof(tfb_noalloc_scratch)];',
+         '// Scratch of the allocation-free entry point: the work counter that CTAs pull',
+         '// tiles from (one word used of TFB_NOALLOC_SCRATCH_WORDS). Every GPU that loads this',
+         '// library keeps one copy until the process exits. All calls share it and it keeps',
+         '// the last call\'s value; each call clears it on its stream before the kernel, so',
+         '// calls ordered on the GPU are independent, and calls that overlap on the GPU',
+         '// (different streams, no ordering between them) race on it.',
+         f'static __device__ __align__(256) unsigned tfb_noalloc_scratch_{n}[TFB_NOALLOC_SCRATCH_WORDS];',
          '',
-         f'__global__ void __launch_bounds__({BT}) kernel_{self.name}_noalloc(const tfb_noalloc_scratch* __restrict__ scr, '
+         f'struct tfb_noalloc_params_{n} {{',
+         '  unsigned num_groups;',
+         f'  unsigned tile_prefix[{G + 1}];',
+         f'  tfb_group_args args[{G}];',
+         '};',
+         '',
+         f'__global__ void __launch_bounds__({BT}) kernel_{n}_noalloc(const __grid_constant__ tfb_noalloc_params_{n} prm, '
          'unsigned* __restrict__ counter) {',
          '  extern __shared__ __align__(16) unsigned char tfb_smem_raw[];',
          f'  {T}* const ubuf = reinterpret_cast<{T}*>(tfb_smem_raw);',
          f'  {T}* const sA = ubuf + {work_vals};',
          '  __shared__ unsigned s_item, s_group, s_tile;',
-         '  const unsigned ngroups = scr->num_groups;',
-         '  const unsigned total = scr->tile_prefix[ngroups];',
+         '  const unsigned ngroups = prm.num_groups;',
+         '  const unsigned total = prm.tile_prefix[ngroups];',
          '  int cur = -1;',
          '  for (;;) {',
          '    if (threadIdx.x == 0) {',
          '      const unsigned item = atomicAdd(counter, 1u);',
          '      unsigned g = 0;',
-         '      while (g + 1u < ngroups && scr->tile_prefix[g + 1u] <= item) ++g;',
-         '      s_item = item; s_group = g; s_tile = item - scr->tile_prefix[g];',
+         '      while (g + 1u < ngroups && prm.tile_prefix[g + 1u] <= item) ++g;',
+         '      s_item = item; s_group = g; s_tile = item - prm.tile_prefix[g];',
          '    }',
          '    __syncthreads();',
          '    const unsigned item = s_item, grp = s_group, tile = s_tile;',
@@ -185,7 +192,7 @@ class GroupedKernel:
          '    if ((int)grp != cur) {',
          '      switch (grp) {']
     for gid in range(G):
-      k.append(f'        case {gid}u: group{gid}_stage_a(scr->args[{gid}], sA); break;')
+      k.append(f'        case {gid}u: group{gid}_stage_a(prm.args[{gid}], sA); break;')
     k += ['        default: break;',
           '      }',
           '      __syncthreads();',
@@ -193,26 +200,33 @@ class GroupedKernel:
           '    }',
           '    switch (grp) {']
     for gid in range(G):
-      k.append(f'      case {gid}u: group{gid}_tile(scr->args[{gid}], (size_t)tile, ubuf, sA); break;')
+      k.append(f'      case {gid}u: group{gid}_tile(prm.args[{gid}], (size_t)tile, ubuf, sA); break;')
     k += ['      default: break;',
           '    }',
           '    __syncthreads();',
           '  }',
           '}',
           '',
-          '// Allocation-free form of tfb_grouped_launch_<set>: the group records are read from host',
-          '// memory (`host_args`, num_groups of them, in group order) and copied into the static',
-          '// scratch on `stream`; the work counter there is cleared by the same copy. Allocates',
-          '// nothing. The first call on a device looks up the scratch address for that device',
-          '// (do it before any stream capture). Returns a cudaError_t value;',
-          '// cudaErrorInvalidValue when num_groups exceeds the fused set or TFB_NOALLOC_MAX_GROUPS.',
-          f'extern "C" int tfb_grouped_launch_noalloc_{self.name}(const void* host_args, unsigned num_groups, void* streamPtr) {{',
+          '// Allocation-free form of tfb_grouped_launch_<set> (declared in',
+          '// tensorforge_b200_grouped.h): `host_args` holds num_groups tfb_group_args records in',
+          '// host memory, in group order; they are passed to the kernel by value, so the caller may',
+          '// reuse that memory as soon as the call returns. Allocates nothing. The first call on a',
+          '// device (the current device) looks up the scratch address there with',
+          '// cudaGetSymbolAddress and keeps it for the process; make that first call before any',
+          '// stream capture. The cached address does not survive cudaDeviceReset. Returns a',
+          '// cudaError_t value: cudaErrorInvalidValue for a null `host_args` or for more groups',
+          '// than the fused set or TFB_NOALLOC_MAX_GROUPS.',
+          f'extern "C" int tfb_grouped_launch_noalloc_{n}(const void* host_args, unsigned num_groups, void* streamPtr) {{',
           f'  static const unsigned tiles_per_group[{G}] = {{{te}}};',
           '  static void* scratch_ptr[64];',
           '  static std::mutex setup_mu;',
           '  cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);',
-          f'  if (num_groups > {G}u || num_groups > TFB_NOALLOC_MAX_GROUPS || host_args == nullptr) {{',
-          f'    std::fprintf(stderr, "tfb_grouped_launch_noalloc_{self.name}: %u groups requested, at most {min(G, 64)} supported\\n", num_groups);',
+          '  if (host_args == nullptr) {',
+          f'    std::fprintf(stderr, "tfb_grouped_launch_noalloc_{n}: host_args is null\\n");',
+          '    return (int)cudaErrorInvalidValue;',
+          '  }',
+          f'  if (num_groups > {G}u || num_groups > TFB_NOALLOC_MAX_GROUPS) {{',
+          f'    std::fprintf(stderr, "tfb_grouped_launch_noalloc_{n}: %u groups requested, at most {min(G, 64)} supported\\n", num_groups);',
           '    return (int)cudaErrorInvalidValue;',
           '  }',
           '  if (num_groups == 0) return 0;',
@@ -224,35 +238,33 @@ class GroupedKernel:
           '    std::lock_guard<std::mutex> guard(setup_mu);',
           '    if (scratch_ptr[device] == nullptr) {',
           '      void* p = nullptr;',
-          '      err = cudaGetSymbolAddress(&p, tfb_noalloc_scratch_storage);',
+          f'      err = cudaGetSymbolAddress(&p, tfb_noalloc_scratch_{n});',
           '      if (err != cudaSuccess) return (int)err;',
           '      scratch_ptr[device] = p;',
           '    }',
           '  }',
-          '  tfb_noalloc_scratch host{};',
-          '  host.counter = 0u;',
-          '  host.num_groups = num_groups;',
+          f'  tfb_noalloc_params_{n} prm{{}};',
+          '  prm.num_groups = num_groups;',
           '  const tfb_group_args* ga = static_cast<const tfb_group_args*>(host_args);',
           '  unsigned long long total = 0;',
           '  for (unsigned g = 0; g < num_groups; ++g) {',
-          '    host.args[g] = ga[g];',
-          '    host.tile_prefix[g] = (unsigned)total;',
+          '    prm.args[g] = ga[g];',
+          '    prm.tile_prefix[g] = (unsigned)total;',
           '    total += (ga[g].num_elements + tiles_per_group[g] - 1) / tiles_per_group[g];',
+          '    if (total > 0xFFFFFFF0ull) return (int)cudaErrorInvalidValue;',
           '  }',
-          '  if (total > 0xFFFFFFF0ull) return (int)cudaErrorInvalidValue;',
-          '  host.tile_prefix[num_groups] = (unsigned)total;',
+          '  prm.tile_prefix[num_groups] = (unsigned)total;',
           '  if (total == 0) return 0;',
-          '  // pageable source: the copy is staged before this call returns, so `host` may go',
-          '  err = cudaMemcpyAsync(scratch_ptr[device], &host, sizeof(host), cudaMemcpyHostToDevice, stream);',
+          '  unsigned* counter = static_cast<unsigned*>(scratch_ptr[device]);',
+          '  err = cudaMemsetAsync(counter, 0, sizeof(unsigned), stream);',
           '  if (err != cudaSuccess) return (int)err;',
           '  int sms = 0, per = 0;',
           '  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);',
-          f'  cudaFuncSetAttribute(kernel_{self.name}_noalloc, cudaFuncAttributeMaxDynamicSharedMemorySize, {self.smem});',
-          f'  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel_{self.name}_noalloc, {BT}, {self.smem});',
+          f'  cudaFuncSetAttribute(kernel_{n}_noalloc, cudaFuncAttributeMaxDynamicSharedMemorySize, {self.smem});',
+          f'  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel_{n}_noalloc, {BT}, {self.smem});',
           '  unsigned grid = (unsigned)((per > 0 ? per : 1) * (sms > 0 ? sms : 1));',
           '  if (grid > total) grid = (unsigned)total;',
-          '  tfb_noalloc_scratch* scr = static_cast<tfb_noalloc_scratch*>(scratch_ptr[device]);',
-          f'  kernel_{self.name}_noalloc<<<grid, {BT}, {self.smem}, stream>>>(scr, &scr->counter);',
+          f'  kernel_{n}_noalloc<<<grid, {BT}, {self.smem}, stream>>>(prm, counter);',
           '  return (int)cudaGetLastError();',
           '}']
     return k

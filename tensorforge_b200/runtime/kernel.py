@@ -1,7 +1,9 @@
 """Load a generated launcher and call it through its C ABI (ctypes), with torch buffers.
 
-The call goes to exactly the symbol a C or C++ caller would link against:
-`launcher_<kernel name>(...)` with the reference's parameter list. Pointer arguments
+The call goes to `tfb_launch_<kernel name>(...)`, the `extern "C"` twin that every
+generated library exports beside the reference-named C++ launcher
+`launcher_<kernel name>(...)`: the same parameter list, with the launch's CUDA status
+as the return value (ctypes cannot bind a C++-mangled name). Pointer arguments
 accept torch tensors (their `data_ptr()`), raw integer addresses or None; pointer
 arrays for PTR_BASED operands are device tensors of int64 addresses; `streamPtr`
 accepts a torch.cuda.Stream, a raw cudaStream_t or None (the current torch stream).
@@ -59,16 +61,15 @@ class CompiledKernel:
       if not os.path.exists(self.so_path):
         raise LaunchError(f'kernel library missing: {self.so_path}')
       self._lib = ctypes.CDLL(self.so_path, mode=ctypes.RTLD_LOCAL)
-      fn = getattr(self._lib, f'launcher_{self.name}')
+      fn = getattr(self._lib, f'tfb_launch_{self.name}')
       fn.argtypes = [_ctype(t) for t, _ in self.params]
-      fn.restype = None
+      fn.restype = ctypes.c_int
       self._fn = fn
-      self._status = self._lib.tensorforge_last_status
-      self._status.restype = ctypes.c_int
     return self._fn
 
   def address(self):
-    """Address of the launcher function (for C callers that receive a function pointer)."""
+    """Address of the status-returning entry point (for C callers that receive a function
+    pointer)."""
     self._load()
     return ctypes.cast(self._fn, ctypes.c_void_p).value
 
@@ -102,8 +103,7 @@ class CompiledKernel:
         if v is None:
           raise TypeError(f'missing argument {name}')
         out.append(v)
-    fn(*out)
-    status = self._status()
+    status = fn(*out)
     if status != 0:
       raise LaunchError(f'launcher_{self.name} failed with CUDA error {status}')
 

@@ -1,6 +1,7 @@
 """Expand the reference's GEMM YAML test suites into concrete cases (tests/golden/gemm_suites.json).
 
 Usage: python tests/golden/make_gemm_suites.py [reference root]
+(default: oracle.ref_omp.REFERENCE_ROOT, i.e. $TFB_REFERENCE_ROOT or the recipe's checkout)
 
 Reads tests/gemms/testsuites/*.yaml of the reference. A value written as a string that
 contains "param" and names a list of the suite is a parameter; a suite's cases are the product of its parameter
@@ -17,6 +18,7 @@ import sys
 import yaml
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 KEEP = 12
 
 
@@ -72,7 +74,8 @@ def expand(spec):
 
 
 def main():
-  root = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+  from oracle.ref_omp import REFERENCE_ROOT
+  root = sys.argv[1] if len(sys.argv) > 1 else REFERENCE_ROOT
   suite_dir = os.path.join(root, 'tests', 'gemms', 'testsuites')
   out = []
   for fn in sorted(os.listdir(suite_dir)):

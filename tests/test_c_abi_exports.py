@@ -65,6 +65,30 @@ def test_generated_launcher_exports_reference_name():
   from tensorforge_b200.runtime.build import build_library
   g = make('c0_gemm_ptr', 'float')
   lib = ctypes.CDLL(build_library(g.get_source()), mode=ctypes.RTLD_LOCAL)
-  assert hasattr(lib, f'launcher_{g.get_base_name()}')
-  assert hasattr(lib, f'tfb_launch_{g.get_base_name()}')  # the status-returning form
+  assert not hasattr(lib, f'launcher_{g.get_base_name()}')  # C++ linkage: the name is mangled
+  assert hasattr(lib, f'tfb_launch_{g.get_base_name()}')  # the status-returning C form
   assert hasattr(lib, 'tensorforge_last_status')
+
+
+def test_reference_declaration_links_against_generated_library(tmp_path):
+  """A C++ caller written against the reference's header (tensorforge/generators/
+  generator.py:198-199: `void launcher_<name>(...);`, C++ linkage, no extern "C")
+  links against the generated library unchanged. Link only, no GPU call."""
+  import shutil
+  import subprocess
+  from tensorforge_b200.kernels import make
+  from tensorforge_b200.runtime.build import build_library
+  g = make('c0_gemm_ptr', 'float')
+  so = build_library(g.get_source())
+  args = ['nullptr' if '*' in t else '0' for t, _ in g.abi_params()]
+  (tmp_path / 'caller.cpp').write_text(
+    '#include <cstddef>\n' + g.get_header() +
+    'int main(int argc, char**) {\n'
+    f'  if (argc > 99) launcher_{g.get_base_name()}({", ".join(args)});\n'
+    '  return 0;\n}\n')
+  cxx = shutil.which('g++')
+  if cxx is None:
+    pytest.skip('g++ not found')
+  r = subprocess.run([cxx, str(tmp_path / 'caller.cpp'), so, '-o', str(tmp_path / 'caller'),
+                      '-Wl,--unresolved-symbols=ignore-in-shared-libs'], capture_output=True, text=True)
+  assert r.returncode == 0, r.stderr[-3000:]

@@ -29,19 +29,22 @@ def test_kernel_name_and_prototype_match_reference(path):
   assert proto == meta['header']
 
 
-def test_header_has_c_linkage_and_defaults():
+def test_header_has_reference_linkage_and_defaults():
+  """The launcher keeps the reference's C++ linkage (generator.py:198-199, :426-436);
+  the status-returning twin has C linkage for FFI callers."""
   g = _gen('c0_gemm_ptr')
   g.generate()
   h = g.get_header()
-  assert h.startswith('extern "C" void launcher_kernel_')
+  assert h.startswith('void launcher_kernel_')
   assert 'unsigned* flags = nullptr, void* streamPtr = nullptr);' in h
   launcher = g.get_launcher()
-  assert launcher.count(f'extern "C" void launcher_{g.get_base_name()}(') == 1
+  assert launcher.count(f'void launcher_{g.get_base_name()}(') == 1
+  assert 'extern "C" void launcher_' not in launcher
   # the status-returning entry point follows the launcher, same parameters without defaults
   params = g._generate_launcher_proto(with_defaults=False).split('(', 1)[1]
   assert f'extern "C" int tfb_launch_{g.get_base_name()}({params} {{' in launcher
   assert 'nullptr' not in launcher.split('tfb_launch_')[1].split('{')[0]
-  assert g.get_status_header() == h.replace('extern "C" void launcher_', 'extern "C" int tfb_launch_')
+  assert g.get_status_header() == 'extern "C" ' + h.replace('void launcher_', 'int tfb_launch_')
 
 
 def test_call_sites():

@@ -105,7 +105,7 @@ def test_legacy_chain_generates_call_site_and_routine(tmp_path):
   writer = cache.routines[g.get_base_name()]
   path = tmp_path / 'subroutine.cu'
   header = writer('r', str(path))
-  assert header.startswith('extern "C" void launcher_')
+  assert header.startswith('void launcher_')
   text = path.read_text()
   assert f'launcher_{g.get_base_name()}' in text and '__global__' in text
   c = Cpp()
