@@ -34,6 +34,10 @@ METRIC = 'order-6 chain elements/s: split-TC vs plain FP32, same B200, rel errâ‰
 CASE = 'chain_o6'
 WORKLOAD = 'order-6 volume chain: out(56x9) = sum_3 K(56x56, 45% sparse) Q(56x9) S(9x9, 24 nnz), FP32'
 FALLBACK_HBM = 6650.0
+# Elements per call of the reference's OpenMP kernel in both CPU legs (the `cpu_baseline`
+# of the headline line and every step of `--impl reference`): a bounded sample of the
+# 500,000-element workload, ~1.3 s per call on 16 host cores.
+CPU_SAMPLE = 4096
 
 
 def log(*a):
@@ -236,19 +240,64 @@ def _cpu_bench(args_list):
   return json.loads(proc.stdout.strip().splitlines()[-1])
 
 
-def reference_cpu(n_target_s=8.0):
-  """The reference's OpenMP-backend chain kernel on all host cores, bounded sample."""
+def reference_cpu(steps=3):
+  """The reference's OpenMP-backend chain kernel on all host cores: `steps` calls of
+  CPU_SAMPLE elements after one warm-up call (mean rate)."""
   from oracle import baseline
   tag = 'bench_chain_o6_float'
   if not baseline.available(tag):
     return None
-  r = _cpu_bench(['--tag', tag, '--case', CASE, '--seconds', str(n_target_s)])
+  r = _cpu_bench(['--tag', tag, '--case', CASE, '--fixed', str(CPU_SAMPLE), '--steps', str(steps), '--warmup', '1'])
   if r is None:
     return None
   return {'value': r['elements_per_s'], 'unit': 'elements/s', 'cores': r['cores'], 'kind': 'reference',
-          'sample': f'{r["elements"]} elements of the 500,000-element workload, one call of the reference '
-                    f'OpenMP-backend kernel (g++ -O3 -march=native -fopenmp, host fallback), '
-                    f'{r["times"][0]:.1f} s'}
+          'sample': f'{CPU_SAMPLE} elements of the 500,000-element workload per call, mean of {steps} calls '
+                    f'after one warm-up, reference OpenMP-backend kernel (g++ -O3 -march=native -fopenmp, '
+                    f'host fallback) on all host threads'}
+
+
+def reference_cpu_c0(n=10000, steps=5):
+  """Config 0 as the reference runs it: its OpenMP-backend GEMM kernel (56x56 * 56x9,
+  pointer arrays, 10,000 elements: the full workload), median of `steps` calls after one
+  warm-up, all host cores."""
+  from oracle import baseline
+  tag = 'bench_c0_gemm_ptr_float'
+  if not baseline.available(tag):
+    return None
+  r = _cpu_bench(['--tag', tag, '--case', 'c0_gemm_ptr', '--fixed', str(n), '--steps', str(steps), '--warmup', '1'])
+  if r is None:
+    return None
+  return {'value': r['elements_per_s_median'], 'unit': 'elements/s', 'cores': r['cores'], 'kind': 'reference',
+          'median_s': r['median_s'],
+          'sample': f'the full {n}-element workload per call, median of {steps} calls after one warm-up, '
+                    'reference OpenMP-backend kernel on all host threads'}
+
+
+def reference_cpu_mixed(groups, sample=512, steps=3):
+  """Config 3 on the host: the reference's OpenMP-backend kernel of every group (one
+  launcher per shape, as the reference runs mixed shapes), each timed on `sample`
+  elements (mean of `steps` calls after one warm-up); the workload's time is the sum over
+  groups of elements / rate."""
+  from oracle import baseline
+  per, total_s, total_el, cores = [], 0.0, 0, None
+  for b, q, n in groups:
+    tag = baseline.mixed_tag(b, q)
+    if not baseline.available(tag):
+      return None
+    r = _cpu_bench(['--tag', tag, '--case', f'mixed_{b}_{q}', '--fixed', str(sample), '--steps', str(steps),
+                    '--warmup', '1'])
+    if r is None:
+      return None
+    cores = r['cores']
+    per.append({'basis': b, 'quantities': q, 'elements_per_s': r['elements_per_s'], 'elements': n,
+                'workload_s': n / r['elements_per_s']})
+    total_s += n / r['elements_per_s']
+    total_el += n
+  return {'value': total_el / total_s, 'unit': 'elements/s', 'cores': cores, 'kind': 'reference',
+          'workload_s': total_s, 'per_group': per,
+          'sample': f'{sample} elements per group and call, mean of {steps} calls after one warm-up, '
+                    'reference OpenMP-backend kernel of each group on all host threads; workload time = '
+                    'sum over groups of elements / rate'}
 
 
 def impl_reference(args, rank, world):
@@ -259,7 +308,7 @@ def impl_reference(args, rank, world):
   if not baseline.available(tag):
     print(json.dumps({'impl': 'reference', 'unavailable': 'reference OpenMP build missing (oracle/_ref)'}))
     return
-  n = args.ref_sample
+  n = CPU_SAMPLE
   r = _cpu_bench(['--tag', tag, '--case', CASE, '--fixed', str(n), '--steps', str(args.steps),
                   '--warmup', str(args.warmup)])
   if r is None:
@@ -294,8 +343,9 @@ def fp32_peak_cached():
   return _FP32_PEAK[0]
 
 
-def extra_workloads(stream, short=False):
-  """Secondary BASELINE configs measured next to the headline (device-resident inputs)."""
+def extra_workloads(stream, short=False, cpu=True):
+  """Secondary BASELINE configs measured next to the headline (device-resident inputs);
+  with `cpu`, the reference's OpenMP-backend kernels for configs 0 and 3 on the host."""
   import torch
   from tensorforge_b200 import workloads as cases
   from tensorforge_b200.kernels import make
@@ -329,6 +379,8 @@ def extra_workloads(stream, short=False):
                            'roofline': {'fp32_bound_el_s': fp32 / (flops / n), 'hbm_bound_el_s': hbm / bytes_el,
                                         'frac_of_tighter': (n / (ms / 1e3)) / min(fp32 / (flops / n), hbm / bytes_el),
                                         'bytes_per_element': bytes_el, 'flops_per_element': flops / n}}
+    if n == 10000 and cpu:
+      out[f'c0_gemm_{n}']['cpu_baseline'] = reference_cpu_c0(n)
     if n >= 1000000:
       # the same GEMM on the tensor cores (TF32x3: operand form B, the default for one term,
       # and form U; parity in the GPU tests)
@@ -371,19 +423,37 @@ def extra_workloads(stream, short=False):
   _, per3 = time_launches(pg.replay, stream, 10, 3)
   ms3 = sum(per3) / len(per3)
   per_group = []
+  fp32 = fp32_peak_cached()
+  hbm = peaks()[0]['hbm_gbs'] * 1e9
+  bound_s = 0.0
   for i, (b, q, n) in enumerate(groups):  # the same launch with every other group emptied
     one = gk.prepare([dict(kw, numElements=(kw['numElements'] if j == i else 0)) for j, kw in enumerate(kws)])
     _, pg = time_launches(one.launch, stream, 3, 1)
     g_ms = sum(pg) / len(pg)
-    g_nz = n * gk.gens[i].get_chain().nz_flops_per_element()
+    ch = gk.gens[i].get_chain()
+    g_nz = n * ch.nz_flops_per_element()
+    g_bytes = n * ch.bytes_per_element() + sum(o.storage_size() * 4 for o in ch.shared())
+    # roofline time of the group: the slower of its FP32-pipe time (nz flops) and HBM time
+    g_bound = max(g_nz / fp32, g_bytes / hbm)
+    bound_s += g_bound
     per_group.append({'basis': b, 'quantities': q, 'elements': n, 'ms': g_ms, 'elements_per_s': n / (g_ms / 1e3),
-                      'nz_gflops': g_nz / (g_ms / 1e3) / 1e9})
+                      'nz_gflops': g_nz / (g_ms / 1e3) / 1e9,
+                      'roofline': {'bound': 'fp32' if g_nz / fp32 >= g_bytes / hbm else 'hbm',
+                                   'frac': g_bound / (g_ms / 1e3), 'fp32_frac': g_nz / fp32 / (g_ms / 1e3),
+                                   'hbm_frac': g_bytes / hbm / (g_ms / 1e3)}})
   out['c3_mixed_shapes'] = {'elements': total_el, 'groups': len(groups), 'elements_per_s': total_el / (ms / 1e3),
                             'nz_gflops': nz / (ms / 1e3) / 1e9, 'ms': ms, 'launch': 'one persistent kernel, CUDA graph replay',
                             'separate_launches_ms': ms2, 'separate_elements_per_s': total_el / (ms2 / 1e3),
                             'graph_per_group_ms': ms3, 'graph_per_group_elements_per_s': total_el / (ms3 / 1e3),
                             'graph_per_group': 'one CUDA graph: each group through its own launcher, 4 side streams',
-                            'per_group': per_group}
+                            'per_group': per_group,
+                            'roofline': {'bound': 'sum over groups of max(nz flops / FP32 peak, bytes / HBM)',
+                                         'bound_ms': bound_s * 1e3, 'frac_persistent': bound_s / (ms / 1e3),
+                                         'frac_graph_per_group': bound_s / (ms3 / 1e3),
+                                         'fp32_peak_tflops': fp32 / 1e12, 'hbm_gbs': hbm / 1e9,
+                                         'peak_source': 'FP32: FFMA probe of this run; HBM: measured copy bandwidth'}}
+  if cpu:
+    out['c3_mixed_shapes']['cpu_baseline'] = reference_cpu_mixed(groups)
   # config 2: log-uniform magnitudes through every precision variant, error vs the FP64 oracle
   descrs = cases.build(CASE, cases.ns_from_module('tensorforge_b200'))
   n2 = 100000 if short else 500000
@@ -608,7 +678,8 @@ def impl_ours(args, rank, world, dist):
   link = link_bound(h2d, d2h)
   link['frac'] = link['duplex_ms'] / e_ms
   cpu = reference_cpu() if (world == 1 and not args.no_cpu) else None
-  extras = extra_workloads(stream, short=args.no_cpu) if (world == 1 and not args.no_extras) else None
+  extras = (extra_workloads(stream, short=args.no_cpu, cpu=not args.no_cpu)
+            if (world == 1 and not args.no_extras) else None)
   line = {
     'metric': METRIC, 'value': value, 'unit': 'elements/s', 'n_gpus': world, 'steps': args.steps,
     'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
@@ -737,7 +808,6 @@ def main():
   ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
   ap.add_argument('--variant', default='auto')
   ap.add_argument('--elements', type=int, default=500000)
-  ap.add_argument('--ref-sample', type=int, default=4096)
   ap.add_argument('--no-cpu', action='store_true')
   ap.add_argument('--no-extras', action='store_true')
   ap.add_argument('--workload', default='chain_o6', choices=['chain_o6', 'ew_update', 'mixed'],

@@ -61,7 +61,9 @@ def main():
     n = (n + 7) // 8 * 8
     times = timed(n, a.steps)
   cores = len(os.sched_getaffinity(0)) if hasattr(os, 'sched_getaffinity') else os.cpu_count()
+  med = sorted(times)[len(times) // 2]
   print(json.dumps({'elements': n, 'times': times, 'elements_per_s': n / (sum(times) / len(times)),
+                    'median_s': med, 'elements_per_s_median': n / med,
                     'cores': cores, 'omp_threads': os.environ.get('OMP_NUM_THREADS', 'all')}))
 
 

@@ -101,26 +101,43 @@ def _wrapper(header, base, fp):
     '}\n')
 
 
-def build(tag, descr_builder, fp='float', opt='-O3', force=False):
-  """Generate + compile one reference OpenMP kernel into oracle/_ref/<tag>.so."""
+def generate_source(tag, descr_builder, fp='float'):
+  """Run the reference generator for one case and write oracle/_ref/<tag>.cpp and .meta
+  (the metadata file is written only once the library is built)."""
   os.makedirs(REF_OUT, exist_ok=True)
-  so = os.path.join(REF_OUT, f'{tag}.so')
-  meta = os.path.join(REF_OUT, f'{tag}.meta')
-  if os.path.exists(so) and os.path.exists(meta) and not force:
-    return so
   kernel, launcher, header, base, mults = generate(descr_builder, fp)
   src = os.path.join(REF_OUT, f'{tag}.cpp')
   with open(src, 'w') as f:
     f.write('#include <omp.h>\n#include <cstddef>\n#include <stdexcept>\n#include <cmath>\n')
     f.write('#include "tensorforge_aux.h"\n\n')
     f.write(kernel + '\n' + launcher + '\n' + _wrapper(header, base, fp))
+  with open(os.path.join(REF_OUT, f'{tag}.pending'), 'w') as f:
+    f.write(f'{base}\n{mults}\n{header}')
+  return src
+
+
+def compile_source(tag, opt='-O3'):
+  """Compile oracle/_ref/<tag>.cpp with the reference's host runtime into <tag>.so."""
+  src = os.path.join(REF_OUT, f'{tag}.cpp')
+  so = os.path.join(REF_OUT, f'{tag}.so')
   inc = os.path.join(REFERENCE_ROOT, 'tensorforge', 'include')
   aux = os.path.join(inc, 'tensorforge_aux_target.cpp')
-  cmd = ['g++', opt, '-march=native', '-fopenmp', '-fPIC', '-shared', f'-I{inc}', src, aux, '-o', so]
+  tmp = so + f'.{os.getpid()}.tmp'
+  cmd = ['g++', opt, '-march=native', '-fopenmp', '-fPIC', '-shared', f'-I{inc}', src, aux, '-o', tmp]
   subprocess.run(cmd, check=True)
-  with open(meta, 'w') as f:
-    f.write(f'{base}\n{mults}\n{header}')
+  os.replace(tmp, so)
+  os.replace(os.path.join(REF_OUT, f'{tag}.pending'), os.path.join(REF_OUT, f'{tag}.meta'))
   return so
+
+
+def build(tag, descr_builder, fp='float', opt='-O3', force=False):
+  """Generate + compile one reference OpenMP kernel into oracle/_ref/<tag>.so."""
+  so = os.path.join(REF_OUT, f'{tag}.so')
+  meta = os.path.join(REF_OUT, f'{tag}.meta')
+  if os.path.exists(so) and os.path.exists(meta) and not force:
+    return so
+  generate_source(tag, descr_builder, fp)
+  return compile_source(tag, opt)
 
 
 class RefKernel:

@@ -5,7 +5,8 @@ stage the lanes split the destination entries (d = lane, lane+G, ...) and each e
 accumulates its full contraction over the contracted index box, contracted index k0
 fastest as in the reference's linearized loop (multilinear.py:105-157). Sparse operands
 are expanded once into dense shared-memory boxes (shared ones once per CTA, batched
-ones once per element), temporaries live in per-element shared memory, and the
+ones once per element), temporaries live in per-element shared memory (regions whose
+live ranges are disjoint share memory: `live_ranges`, `assign_offsets`), and the
 destination is updated in global memory stage by stage, exactly in descriptor order.
 The grid loops over element tiles, so the same kernel also runs persistently.
 """
@@ -34,20 +35,108 @@ def _sparse_box(op):
   return shape
 
 
-def smem_layout(chain):
-  """(values in the CTA-shared region, values per element) for the generic generator."""
-  shared = 0
-  for o in chain.operands:
-    if o.kind == 'shared' and o.sparse:
-      shared += _prod(_sparse_box(o))
-  per_elem = 0
+def _stage_access(st):
+  """(operands written, operands read) by one stage, as sets of operand ids."""
+  if getattr(st, 'kind', '') == 'elementwise':
+    return {id(o) for o in st.written}, {id(o) for o in st.read}
+  reads = {id(r.op) for r in st.ops}
+  if st.add:
+    reads.add(id(st.dest))
+  return {id(st.dest)}, reads
+
+
+def live_ranges(chain):
+  """Live interval [first, last] (stage indices) of every per-element shared-memory region:
+  batched sparse operands (expanded right before the first stage reading them, live until
+  the last one) and temporaries (from the first stage writing them to the last stage
+  touching them). Restates the reference's liveness analysis (backend/opt/liveness.py:
+  12-57) over this IR's stages."""
+  access = [_stage_access(st) for st in chain.stages]
+  out = {}
   for o in chain.operands:
     if o.kind == 'batched' and o.sparse:
-      per_elem += _prod(_sparse_box(o))
+      used = [i for i, (_, r) in enumerate(access) if id(o) in r]
+      out[o.name] = (min(used), max(used)) if used else (0, 0)
   for t in chain.tmps:
-    per_elem += max([s.defines_volume(t) for s in chain.stages] + [0])
-  # keep every region 16-byte aligned for vector accesses
-  return _align4(shared), _align4(per_elem)
+    touched = [i for i, (w, r) in enumerate(access) if id(t) in w or id(t) in r]
+    written = [i for i, (w, _) in enumerate(access) if id(t) in w]
+    first = min(written) if written else (min(touched) if touched else 0)
+    out[t.name] = (first, max(touched) if touched else first)
+  return out
+
+
+def region_sizes(chain):
+  """Values per element of every per-element region (expanded sparse box or temporary),
+  each rounded up to a multiple of 4 so that every region stays 16-byte aligned."""
+  sizes = {}
+  for o in chain.operands:
+    if o.kind == 'batched' and o.sparse:
+      sizes[o.name] = _align4(_prod(_sparse_box(o)))
+  for t in chain.tmps:
+    sizes[t.name] = _align4(max([s.defines_volume(t) for s in chain.stages] + [0]))
+  return sizes
+
+
+def assign_offsets(sizes, ranges):
+  """Offsets (values) for regions whose live intervals may share memory: two regions
+  overlap in memory only if their intervals are disjoint. First fit in order of interval
+  start (largest first on ties) over an interval graph - the reference's region allocation
+  (backend/opt/mem_region_allocation.py:29-94, coloring/coloring.py:24-96) colours the
+  same interference relation and sizes each colour by its largest member; first fit by
+  offset packs regions of different sizes tighter. Returns ({name: offset}, total)."""
+  placed = []
+  offsets = {}
+  for name in sorted(sizes, key=lambda n: (ranges[n][0], -sizes[n], n)):
+    lo, hi = ranges[name]
+    busy = sorted((offsets[p], offsets[p] + sizes[p]) for p in placed
+                  if not (ranges[p][1] < lo or hi < ranges[p][0]))
+    off = 0
+    for a, b in busy:
+      if off + sizes[name] <= a:
+        break
+      off = max(off, b)
+    offsets[name] = off
+    placed.append(name)
+  total = max([offsets[n] + sizes[n] for n in sizes] + [0])
+  return offsets, _align4(total)
+
+
+def shared_regions(chain):
+  """CTA-shared regions (expanded shared sparse operands): ({name: offset}, total values,
+  {names expanded once per CTA}). Operands whose memory no other region uses are expanded
+  once per CTA; when the resident layout would not fit next to the per-element regions,
+  operands with disjoint live ranges share memory and are expanded again, per tile, right
+  before the first stage reading them."""
+  ops = [o for o in chain.operands if o.kind == 'shared' and o.sparse]
+  sizes = {o.name: _align4(_prod(_sparse_box(o))) for o in ops}
+  resident_total = sum(sizes.values())
+  offsets, off = {}, 0
+  for o in ops:
+    offsets[o.name] = off
+    off += sizes[o.name]
+  _, per_elem = assign_offsets(region_sizes(chain), live_ranges(chain))
+  if (resident_total + per_elem) * chain.fp.size() <= 227 * 1024 or len(ops) < 2:
+    return offsets, resident_total, {o.name for o in ops}
+  access = [_stage_access(st) for st in chain.stages]
+  ranges = {}
+  for o in ops:
+    used = [i for i, (_, r) in enumerate(access) if id(o) in r]
+    ranges[o.name] = (min(used), max(used)) if used else (0, 0)
+  offsets, total = assign_offsets(sizes, ranges)
+  resident = set()
+  for n in sizes:
+    lo, hi = offsets[n], offsets[n] + sizes[n]
+    if not any(m != n and offsets[m] < hi and lo < offsets[m] + sizes[m] for m in sizes):
+      resident.add(n)
+  return offsets, total, resident
+
+
+def smem_layout(chain):
+  """(values in the CTA-shared region, values per element) for the generic generator,
+  with regions reusing memory across disjoint live ranges."""
+  _, shared, _ = shared_regions(chain)
+  _, per_elem = assign_offsets(region_sizes(chain), live_ranges(chain))
+  return shared, per_elem
 
 
 def _align4(x):
@@ -89,22 +178,16 @@ class GenericEmitter:
   # ---------------------------------------------------------------- layout
   def _regions(self):
     regions = {}
-    off = 0
+    soff, shared, self.resident = shared_regions(self.chain)
     for o in self.chain.operands:
       if o.kind == 'shared' and o.sparse:
-        regions[o.name] = ('shared', off, _sparse_box(o))
-        off += _prod(_sparse_box(o))
-    shared = _align4(off)
-    off = 0
+        regions[o.name] = ('shared', soff[o.name], _sparse_box(o))
+    offsets, per_elem = assign_offsets(region_sizes(self.chain), live_ranges(self.chain))
     for o in self.chain.operands:
       if o.kind == 'batched' and o.sparse:
-        regions[o.name] = ('elem', off, _sparse_box(o))
-        off += _prod(_sparse_box(o))
+        regions[o.name] = ('elem', offsets[o.name], _sparse_box(o))
     for t in self.chain.tmps:
-      vol = max([s.defines_volume(t) for s in self.chain.stages] + [0])
-      regions[t.name] = ('elem', off, None)
-      off += vol
-    per_elem = _align4(off)
+      regions[t.name] = ('elem', offsets[t.name], None)
     return regions, shared, per_elem
 
   # ---------------------------------------------------------------- access
@@ -188,18 +271,14 @@ class GenericEmitter:
     for o in chain.operands:
       if o.kind == 'data' and len(o.shape) > 0:
         self.w(f'const {T}* const data_{o.name} = data_{o.name}_{self.base};')
-    # shared sparse operands expanded once per CTA
+    # shared sparse operands: resident ones expanded once per CTA, the others (sharing
+    # memory with another shared region) per tile before their first stage
     for o in chain.operands:
       if o.kind == 'shared' and o.sparse:
         _, off, box = regions[o.name]
-        vol = _prod(box)
-        nnz = len(o.nonzeros())
         self.w(f'{T}* const dn_{o.name} = tfb_smem + {off};')
-        with self.block(f'for (unsigned i = threadIdx.x; i < {vol}u; i += blockDim.x)'):
-          self.w(f'dn_{o.name}[i] = {self.lit(0)};')
-        self.w('__syncthreads();')
-        with self.block(f'for (unsigned i = threadIdx.x; i < {nnz}u; i += blockDim.x)'):
-          self.w(f'dn_{o.name}[scat_{o.name}_{self.base}[i]] = {o.name}[spos_{o.name}_{self.base}[i]];')
+        if o.name in self.resident:
+          self._expand_shared(o, box)
     self.w('__syncthreads();')
     self.w(f'const unsigned slot = threadIdx.x / {G}u;')
     self.w(f'const unsigned lane = threadIdx.x % {G}u;')
@@ -225,23 +304,29 @@ class GenericEmitter:
           self.w(f'{const}{T}* const glb_{o.name} = active ? {o.name} + batchId * {o.element_volume()}u + {o.name}_extraOffset : nullptr;')
         else:
           self.w(f'{const}{T}* const glb_{o.name} = active ? {o.name}[batchId] + {o.name}_extraOffset : nullptr;')
-      # expand batched sparse operands
-      any_sparse = False
-      for o in chain.operands:
-        if o.kind == 'batched' and o.sparse:
-          any_sparse = True
-          _, off, box = regions[o.name]
-          with self.block(f'for (unsigned i = lane; i < {_prod(box)}u; i += {G}u)'):
-            self.w(f'dn_{o.name}[i] = {self.lit(0)};')
-      if any_sparse:
-        self.w(f'{sync};')
-        for o in chain.operands:
-          if o.kind == 'batched' and o.sparse:
+      first_use = live_ranges(chain)
+      for si, st in enumerate(chain.stages):
+        # batched sparse operands are expanded right before the first stage that reads them
+        # (their region may reuse the memory of regions that are dead by then)
+        shared_now = [o for o in chain.operands if o.kind == 'shared' and o.sparse and o.name not in self.resident
+                      and min([i for i, (_, r) in enumerate(map(_stage_access, chain.stages)) if id(o) in r] + [0]) == si]
+        if shared_now:
+          self.w('__syncthreads();  // every element group is done with the region\'s previous operand')
+          for o in shared_now:
+            self._expand_shared(o, regions[o.name][2])
+          self.w('__syncthreads();')
+        expand = [o for o in chain.operands if o.kind == 'batched' and o.sparse and first_use[o.name][0] == si]
+        if expand:
+          for o in expand:
+            _, off, box = regions[o.name]
+            with self.block(f'for (unsigned i = lane; i < {_prod(box)}u; i += {G}u)'):
+              self.w(f'dn_{o.name}[i] = {self.lit(0)};')
+          self.w(f'{sync};')
+          for o in expand:
             nnz = len(o.nonzeros())
             with self.block(f'if (active) for (unsigned i = lane; i < {nnz}u; i += {G}u)'):
               self.w(f'dn_{o.name}[scat_{o.name}_{self.base}[i]] = glb_{o.name}[spos_{o.name}_{self.base}[i]];')
-        self.w(f'{sync};')
-      for si, st in enumerate(chain.stages):
+          self.w(f'{sync};')
         self.w(f'// stage {si}: {st.descr}'.replace('\n', ' '))
         with self.block('if (active)'):
           if getattr(st, 'kind', '') == 'elementwise':
@@ -252,6 +337,16 @@ class GenericEmitter:
     self.ind -= 1
     self.w('}')
     return '\n'.join(self.lines)
+
+  def _expand_shared(self, o, box):
+    """Zero the dense box of shared sparse operand `o` and scatter its nonzeros (all CTA threads)."""
+    vol = _prod(box)
+    nnz = len(o.nonzeros())
+    with self.block(f'for (unsigned i = threadIdx.x; i < {vol}u; i += blockDim.x)'):
+      self.w(f'dn_{o.name}[i] = {self.lit(0)};')
+    self.w('__syncthreads();')
+    with self.block(f'for (unsigned i = threadIdx.x; i < {nnz}u; i += blockDim.x)'):
+      self.w(f'dn_{o.name}[scat_{o.name}_{self.base}[i]] = {o.name}[spos_{o.name}_{self.base}[i]];')
 
   def _meta(self):
     out = ['// meta data:']

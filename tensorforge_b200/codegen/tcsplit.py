@@ -195,6 +195,10 @@ def plan(chain, shape, precision, variant):
   params = {'precision': precision, 'chunk': chunk, 'pipe': pipe}
   if int(variant.get('ahead', 0)) and pipe == 2:
     params['ahead'] = 1
+  if int(variant.get('wait_probe', 0)) > 0:
+    # failure-detection check: the kernel first waits, with this many polls, on an mbarrier
+    # that nothing arrives on, records error 30 and returns before issuing any copy or MMA
+    params['wait_probe'] = int(variant['wait_probe'])
   return Plan('tcsplit', params, smem, 32 * (4 * H_GROUPS + 1),
               note=f'M={shape.M} N={shape.N} terms={len(shape.terms)} tmem={lay["tmem_used"]} smem={sm["total"]}')
 
@@ -458,6 +462,10 @@ class _TC:
     nbars = 2 * nterms + (3 if self.pipe == 2 else 2)
     BAR_STAGE = 2 * nterms + 2
     self.w(f'unsigned* const tmem_slot = reinterpret_cast<unsigned*>(bars + {nbars});')
+    probe = int(self.plan.params.get('wait_probe', 0))
+    if probe:
+      self.w(f'uint64_t* const probe_bar = bars + {nbars + 1};  // never arrived on')
+      assert (nbars + 2) * 8 <= 256
     if self.pipe == 2:
       self.w(f'float* const stage = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_stage"]});')
       for ti in range(nterms):
@@ -499,6 +507,8 @@ class _TC:
     if self.pipe == 2:
       # one arrival per producer (cp.async completion) + the bulk-copy issuer's expect_tx
       self.w(f'tfb_tc::mbar_init(&bars[{BAR_STAGE}], {NP + 1}u);')
+    if probe:
+      self.w('tfb_tc::mbar_init(probe_bar, 1u);')
     self.w('asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");')
     self.close()
     self.open('if (warp == 0)')
@@ -510,6 +520,11 @@ class _TC:
     self.w('tfb_tc::fence_after();')
     self.w('const unsigned tmem = *tmem_slot;')
     self.w('bool ok = true;')
+    if probe:
+      # nothing has been issued yet: on timeout every thread goes straight to the teardown
+      self.w(f'if (threadIdx.x == 0 && !tfb_tc::mbar_wait(probe_bar, 0u, {probe}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 30u); }}')
+      self.w('ok = __syncthreads_and(ok ? 1 : 0) != 0;')
+      self.open('if (ok)')
     # ---- MMA issuer
     self.open(f'if (warp == {4 * H})')
     self.open('if (lane == 0)')
@@ -590,6 +605,8 @@ class _TC:
       self.close()
       self.w('tfb_tc::cp_async_wait_all();')
       self.w('if (ptid == 0) tfb_tc::bulk_wait();')
+      self.close()
+    if probe:
       self.close()
     # ---- teardown
     self.w('tfb_tc::fence_before();')

@@ -226,6 +226,11 @@ CASES = {
 
 
 def build(name, ns):
+  """Descriptor list of a named case; `mixed_<basis>_<quantities>` names one group of the
+  mixed-shape workload (`mixed_chain`)."""
+  if name.startswith('mixed_') and name not in CASES:
+    _, b, q = name.split('_')
+    return mixed_chain(ns, int(b), int(q))
   fn, kwargs, _ = CASES[name]
   return fn(ns, **kwargs)
 

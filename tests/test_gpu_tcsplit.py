@@ -190,3 +190,37 @@ def test_form_u_split_ahead(n):
       assert np.array_equal(got[s:s + 504], ref[s:s + 504])
     got, ref, _, _ = _run('chain_o6', 'tf32x3', 777, dist='loguniform', variant=dict(FORM_U_AHEAD))
     assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-6
+
+
+def test_bounded_wait_runs_out_and_context_stays_usable():
+  """Failure detection without a fault: a kernel built with a 4,096-poll wait on an
+  mbarrier that nothing arrives on (plan option `wait_probe`, before any copy or MMA is
+  issued) gives up, records error 30 in its error word and returns; the launch itself
+  succeeds, the outputs are untouched, reading the error word clears it, and the regular
+  kernel then runs in the same context and matches the oracle."""
+  import torch
+  from tensorforge_b200.kernels import make
+  from tensorforge_b200.runtime import compile_generator
+  n = 333
+  g = make('chain_o6', 'float', precision='tf32x3', variant={'wait_probe': 4096})
+  assert g.get_plan().params.get('wait_probe') == 4096
+  k = compile_generator(g)
+  descrs = cases.build('chain_o6', cases.ns_from_module('tensorforge_b200'))
+  lay, mem = harness.make_memory(descrs, n, seed=5)
+  dev, kw = {}, {'numElements': n}
+  for l in lay:
+    dev[l.name] = torch.tensor(mem.buffers[l.name], dtype=torch.float32, device='cuda')
+    kw[l.name] = dev[l.name]
+    if l.kind == 'strided':
+      kw[f'{l.name}_extraOffset'] = l.extra_offset
+  out = [l for l in lay if l.kind == 'strided' and l.tensor.direction.name != 'SOURCE'][0]
+  before = dev[out.name].clone()
+  k(**kw)
+  torch.cuda.synchronize()
+  errf = getattr(ctypes.CDLL(k.so_path), f'tfb_kernel_error_{g.get_base_name()}')
+  errf.argtypes = [ctypes.c_void_p]
+  assert errf(None) == 30
+  assert errf(None) == 0  # read and cleared
+  assert torch.equal(dev[out.name], before)
+  got, ref, _, _ = _run('chain_o6', 'tf32x3', n, seed=5)
+  assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-6
