@@ -146,6 +146,20 @@ def smem_plan_v2(shape, precision):
               pitch=pitch, ubuf_bytes=ubuf, off_bar=off_bar, total=total, te=te, tc=tc)
 
 
+def pipe3_ok(shape, precision, chunk=16):
+  """The warp-specialised pipeline (pipe 3) needs TF32 splits, a U pass for every term
+  (K a multiple of 4, lane phases of at most 4 x 16 columns) and tensor memory for two A
+  slots plus two accumulator pairs."""
+  if precision != 'tf32x3' or chunk != 16:
+    return False
+  lay = layout(shape, precision)
+  if any(t.R is None or t.R.kind != 'batched' or t.K % 4 for t in shape.terms):
+    return False
+  if any(-(-kp // 16) > H_GROUPS for kp in lay['kpad']):
+    return False
+  return 4 * max(lay['a_cols']) + 4 * lay['n_mma'] <= 512
+
+
 def plan(chain, shape, precision, variant):
   if precision not in KSTEP:
     return None
@@ -183,8 +197,10 @@ def plan(chain, shape, precision, variant):
   for t in shape.terms:
     if t.R is not None and t.R.kind != 'batched':
       return None
-  pipe = variant.get('pipe', 2)
-  sm = smem_plan_v2(shape, precision) if pipe == 2 else None
+  pipe = variant.get('pipe', 3 if pipe3_ok(shape, precision, variant.get('chunk', 16)) else 2)
+  if pipe == 3 and not pipe3_ok(shape, precision, variant.get('chunk', 16)):
+    pipe = 2
+  sm = smem_plan_v2(shape, precision) if pipe in (2, 3) else None
   if sm is None or sm['total'] > _plan.SMEM_LIMIT:
     pipe = 1
     sm = smem_plan(shape, precision)
@@ -343,7 +359,7 @@ class _TC:
     self.prec = plan_.params['precision']
     self.lay = layout(shape, self.prec)
     self.pipe = plan_.params.get('pipe', 1)
-    self.sm = smem_plan_v2(shape, self.prec) if self.pipe == 2 else smem_plan(shape, self.prec)
+    self.sm = smem_plan_v2(shape, self.prec) if self.pipe in (2, 3) else smem_plan(shape, self.prec)
     self.LC = plan_.params['chunk']
     self.ahead = bool(plan_.params.get('ahead', 0))
     self.H = H_GROUPS
@@ -400,7 +416,7 @@ class _TC:
     for op, vals in staged:
       stage_off[op.name] = off          # floats, within one stage buffer
       off += te * _pad(vals, 4)
-    if self.pipe == 2:
+    if self.pipe in (2, 3):
       stage_off = dict(sm['stage_off'])
     # B operand blocks (hi/lo per term) at the start of shared memory
     ke = 16 // es
@@ -452,21 +468,27 @@ class _TC:
       col += lay['slot_cols'][ti]
     d_main, d_corr = col, col + n_mma
     lim = self.WAIT_LIMIT
-    nthreads = 32 * (4 * H + 1)
+    p3 = self.pipe == 3
+    nthreads = 32 * (4 * H + 1 + (4 if p3 else 0))
     BAR_FULL, BAR_FREE, BAR_DFULL, BAR_DFREE = 0, nterms, 2 * nterms, 2 * nterms + 1
+    if p3:
+      # two A slots used in turn by the terms of consecutive tiles, two accumulator pairs
+      self.scols = 2 * max(lay['a_cols'])
+      self.d_base = 2 * self.scols
+      BAR_FULL, BAR_FREE, BAR_DFULL, BAR_DFREE = 0, 2, 4, 6
 
     self.w(f'__global__ void __launch_bounds__({nthreads}, 1) {kname}({", ".join(self.params(globals_))}) {{')
     self.ind += 1
     self.w('extern __shared__ __align__(1024) unsigned char tfb_smem_raw[];')
     self.w(f'uint64_t* const bars = reinterpret_cast<uint64_t*>(tfb_smem_raw + {sm["off_bar"]});')
-    nbars = 2 * nterms + (3 if self.pipe == 2 else 2)
-    BAR_STAGE = 2 * nterms + 2
+    nbars = 9 if p3 else 2 * nterms + (3 if self.pipe == 2 else 2)
+    BAR_STAGE = 8 if p3 else 2 * nterms + 2
     self.w(f'unsigned* const tmem_slot = reinterpret_cast<unsigned*>(bars + {nbars});')
     probe = int(self.plan.params.get('wait_probe', 0))
     if probe:
       self.w(f'uint64_t* const probe_bar = bars + {nbars + 1};  // never arrived on')
       assert (nbars + 2) * 8 <= 256
-    if self.pipe == 2:
+    if self.pipe in (2, 3):
       self.w(f'float* const stage = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_stage"]});')
       for ti in range(nterms):
         self.w(f'float* const ubuf{ti} = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_u"] + ti * sm["ubuf_bytes"]});')
@@ -499,12 +521,19 @@ class _TC:
         self.w(f'*reinterpret_cast<__nv_bfloat16*>(tfb_smem_raw + {lo_off} + boff) = l;')
       self.close()
     self.open('if (threadIdx.x == 0)')
-    for ti in range(nterms):
-      self.w(f'tfb_tc::mbar_init(&bars[{BAR_FULL + ti}], {NP}u);')
-      self.w(f'tfb_tc::mbar_init(&bars[{BAR_FREE + ti}], 1u);')
-    self.w(f'tfb_tc::mbar_init(&bars[{BAR_DFULL}], 1u);')
-    self.w(f'tfb_tc::mbar_init(&bars[{BAR_DFREE}], {NP}u);')
-    if self.pipe == 2:
+    if p3:
+      for i in range(2):
+        self.w(f'tfb_tc::mbar_init(&bars[{BAR_FULL + i}], {NP}u);')
+        self.w(f'tfb_tc::mbar_init(&bars[{BAR_FREE + i}], 1u);')
+        self.w(f'tfb_tc::mbar_init(&bars[{BAR_DFULL + i}], 1u);')
+        self.w(f'tfb_tc::mbar_init(&bars[{BAR_DFREE + i}], 128u);')
+    else:
+      for ti in range(nterms):
+        self.w(f'tfb_tc::mbar_init(&bars[{BAR_FULL + ti}], {NP}u);')
+        self.w(f'tfb_tc::mbar_init(&bars[{BAR_FREE + ti}], 1u);')
+      self.w(f'tfb_tc::mbar_init(&bars[{BAR_DFULL}], 1u);')
+      self.w(f'tfb_tc::mbar_init(&bars[{BAR_DFREE}], {NP}u);')
+    if self.pipe in (2, 3):
       # one arrival per producer (cp.async completion) + the bulk-copy issuer's expect_tx
       self.w(f'tfb_tc::mbar_init(&bars[{BAR_STAGE}], {NP + 1}u);')
     if probe:
@@ -526,38 +555,44 @@ class _TC:
       self.w('ok = __syncthreads_and(ok ? 1 : 0) != 0;')
       self.open('if (ok)')
     # ---- MMA issuer
-    self.open(f'if (warp == {4 * H})')
-    self.open('if (lane == 0)')
-    self.w('unsigned it = 0;')
-    self.open('for (size_t tile = blockIdx.x; tile < numTiles && ok; tile += gridDim.x, ++it)')
-    self.w(f'if (it > 0 && !tfb_tc::mbar_wait(&bars[{BAR_DFREE}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 13u); break; }}')
-    mma = 'mma_tf32' if prec == 'tf32x3' else 'mma_f16'
-    for ti, t in enumerate(s.terms):
-      kp = lay['kpad'][ti]
-      ksteps = kp // lay['ks']
-      hi_off, lo_off = b_off[ti]
-      sbo = (kp // ke) * 128
-      acols = lay['a_cols'][ti]
-      cps = lay['ks'] * es // 4
-      self.w(f'if (!tfb_tc::mbar_wait(&bars[{BAR_FULL + ti}], it & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, {10 + ti}u); break; }}')
-      self.w('tfb_tc::fence_after();')
-      self.open(f'for (int ks = 0; ks < {ksteps}; ++ks)')
-      self.w(f'const unsigned a_hi = tmem + {slot_base[ti]}u + ks * {cps}u;')
-      self.w(f'const unsigned a_lo = a_hi + {acols}u;')
-      self.w(f'const uint64_t bh = tfb_tc::smem_desc(tfb_tc::smem_u32(tfb_smem_raw + {hi_off}) + ks * 256u, 128u, {sbo}u);')
-      self.w(f'const uint64_t bl = tfb_tc::smem_desc(tfb_tc::smem_u32(tfb_smem_raw + {lo_off}) + ks * 256u, 128u, {sbo}u);')
-      first = '(ks > 0) ? 1u : 0u' if ti == 0 else '1u'
-      self.w(f'tfb_tc::{mma}(tmem + {d_main}u, a_hi, bh, {idesc}u, {first});')
-      self.w(f'tfb_tc::{mma}(tmem + {d_corr}u, a_hi, bl, {idesc}u, {first});')
-      self.w(f'tfb_tc::{mma}(tmem + {d_corr}u, a_lo, bh, {idesc}u, 1u);')
+    if p3:
+      self._mma_v3(s, lay, b_off, ke, es, idesc, lim, n_mma)
+    else:
+      self.open(f'if (warp == {4 * H})')
+      self.open('if (lane == 0)')
+      self.w('unsigned it = 0;')
+      self.open('for (size_t tile = blockIdx.x; tile < numTiles && ok; tile += gridDim.x, ++it)')
+      self.w(f'if (it > 0 && !tfb_tc::mbar_wait(&bars[{BAR_DFREE}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 13u); break; }}')
+      mma = 'mma_tf32' if prec == 'tf32x3' else 'mma_f16'
+      for ti, t in enumerate(s.terms):
+        kp = lay['kpad'][ti]
+        ksteps = kp // lay['ks']
+        hi_off, lo_off = b_off[ti]
+        sbo = (kp // ke) * 128
+        acols = lay['a_cols'][ti]
+        cps = lay['ks'] * es // 4
+        self.w(f'if (!tfb_tc::mbar_wait(&bars[{BAR_FULL + ti}], it & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, {10 + ti}u); break; }}')
+        self.w('tfb_tc::fence_after();')
+        self.open(f'for (int ks = 0; ks < {ksteps}; ++ks)')
+        self.w(f'const unsigned a_hi = tmem + {slot_base[ti]}u + ks * {cps}u;')
+        self.w(f'const unsigned a_lo = a_hi + {acols}u;')
+        self.w(f'const uint64_t bh = tfb_tc::smem_desc(tfb_tc::smem_u32(tfb_smem_raw + {hi_off}) + ks * 256u, 128u, {sbo}u);')
+        self.w(f'const uint64_t bl = tfb_tc::smem_desc(tfb_tc::smem_u32(tfb_smem_raw + {lo_off}) + ks * 256u, 128u, {sbo}u);')
+        first = '(ks > 0) ? 1u : 0u' if ti == 0 else '1u'
+        self.w(f'tfb_tc::{mma}(tmem + {d_main}u, a_hi, bh, {idesc}u, {first});')
+        self.w(f'tfb_tc::{mma}(tmem + {d_corr}u, a_hi, bl, {idesc}u, {first});')
+        self.w(f'tfb_tc::{mma}(tmem + {d_corr}u, a_lo, bh, {idesc}u, 1u);')
+        self.close()
+        self.w(f'tfb_tc::mma_commit(&bars[{BAR_FREE + ti}]);')
+      self.w(f'tfb_tc::mma_commit(&bars[{BAR_DFULL}]);')
       self.close()
-      self.w(f'tfb_tc::mma_commit(&bars[{BAR_FREE + ti}]);')
-    self.w(f'tfb_tc::mma_commit(&bars[{BAR_DFULL}]);')
-    self.close()
-    self.close()
-    self.close()
+      self.close()
+      self.close()
     # ---- producers
-    if self.pipe == 2:
+    if p3:
+      self._producers_v3(s, te, tcols, NP, stage_off, lim, BAR_STAGE)
+      self._epilogue_warps_v3(s, te, tcols, lim, n_mma)
+    elif self.pipe == 2:
       self._producers_v2(s, te, tcols, NP, stage_off, slot_base, lim, BAR_DFULL, BAR_STAGE, d_main, d_corr)
     else:
       self.open(f'else if (warp < {4 * H})')
@@ -853,6 +888,196 @@ class _TC:
     self.w(f'if (pending && !tfb_tc::mbar_wait(&bars[{BAR_STAGE}], it & 1u, {lim}ull)) atomicMax(&tfb_err_{b}, 41u);')
     self.w('tfb_tc::cp_async_wait_all();')
     self.w('if (ptid == 0) tfb_tc::bulk_wait();')
+    self.close()
+
+  # ------------------------------------------------------------------ warp-specialised pipeline
+  # Barriers: FULL[0..1] (A slot written, NP arrivals), FREE[0..1] (A slot read by the MMAs,
+  # one commit), DFULL[0..1] (accumulator pair complete, one commit), DFREE[0..1]
+  # (accumulator pair read, 128 epilogue arrivals), STAGE (inputs landed). Term t of the
+  # CTA's it-th tile is chunk c = it * terms + t and uses A slot c % 2; tile it uses
+  # accumulator pair it % 2.
+  def _mma_v3(self, s, lay, b_off, ke, es, idesc, lim, n_mma):
+    b = self.base
+    nterms = len(s.terms)
+    mma = 'mma_tf32' if self.prec == 'tf32x3' else 'mma_f16'
+    half = self.scols // 2
+    self.open(f'if (warp == {4 * self.H})')
+    self.open('if (lane == 0)')
+    self.w('unsigned it = 0, chunk = 0;')
+    self.open('for (size_t tile = blockIdx.x; tile < numTiles && ok; tile += gridDim.x, ++it)')
+    self.w('const unsigned db = it & 1u;')
+    self.w(f'const unsigned d_main = tmem + {self.d_base}u + db * {2 * n_mma}u, d_corr = d_main + {n_mma}u;')
+    self.w(f'if (it >= 2u && !tfb_tc::mbar_wait(&bars[6u + db], ((it - 2u) >> 1) & 1u, {lim}ull)) '
+           f'{{ ok = false; atomicMax(&tfb_err_{b}, 13u); break; }}')
+    self.w('tfb_tc::fence_after();')
+    for ti, t in enumerate(s.terms):
+      kp = lay['kpad'][ti]
+      ksteps = kp // lay['ks']
+      hi_off, lo_off = b_off[ti]
+      sbo = (kp // ke) * 128
+      cps = lay['ks'] * es // 4
+      self.w('{')
+      self.w('const unsigned sl = chunk & 1u;')
+      self.w(f'if (!tfb_tc::mbar_wait(&bars[sl], (chunk >> 1) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, {10 + ti}u); break; }}')
+      self.w('tfb_tc::fence_after();')
+      self.open(f'for (int ks = 0; ks < {ksteps}; ++ks)')
+      self.w(f'const unsigned a_hi = tmem + sl * {self.scols}u + ks * {cps}u;')
+      self.w(f'const unsigned a_lo = a_hi + {half}u;')
+      self.w(f'const uint64_t bh = tfb_tc::smem_desc(tfb_tc::smem_u32(tfb_smem_raw + {hi_off}) + ks * 256u, 128u, {sbo}u);')
+      self.w(f'const uint64_t bl = tfb_tc::smem_desc(tfb_tc::smem_u32(tfb_smem_raw + {lo_off}) + ks * 256u, 128u, {sbo}u);')
+      first = '(ks > 0) ? 1u : 0u' if ti == 0 else '1u'
+      self.w(f'tfb_tc::{mma}(d_main, a_hi, bh, {idesc}u, {first});')
+      self.w(f'tfb_tc::{mma}(d_corr, a_hi, bl, {idesc}u, {first});')
+      self.w(f'tfb_tc::{mma}(d_corr, a_lo, bh, {idesc}u, 1u);')
+      self.close()
+      self.w('tfb_tc::mma_commit(&bars[2u + sl]);')
+      self.w('++chunk;')
+      self.w('}')
+    self.w('tfb_tc::mma_commit(&bars[4u + db]);')
+    self.close()
+    self.close()
+    self.close()
+
+  def _lane_v3(self, ti, t, lim, src, nterms):
+    """Lane phase of term ti into A slot (chunk % 2): wait until the MMAs of the chunk two
+    before have read the slot, split the lane's column of U_t and store hi / lo."""
+    b = self.base
+    kp = self.lay['kpad'][ti]
+    half = self.scols // 2
+    self.open('')
+    self.w(f'const unsigned chunk = it * {nterms}u + {ti}u, sl = chunk & 1u;')
+    self.w(f'if (chunk >= 2u && !tfb_tc::mbar_wait(&bars[2u + sl], ((chunk - 2u) >> 1) & 1u, {lim}ull)) '
+           f'{{ ok = false; atomicMax(&tfb_err_{b}, {30 + ti}u); }}')
+    self.w('tfb_tc::fence_after();')
+    self.w(f'const unsigned slot = lane_addr + sl * {self.scols}u;')
+    self.w('const unsigned c0 = grp * 16u;')
+    self.open(f'if (c0 < {kp}u)')
+    self.w('float u[16];')
+    self.w('#pragma unroll')
+    self.w('for (int i = 0; i < 16; ++i) u[i] = 0.0f;')
+    self.open('if (active)')
+    self.w(f'const float* p = {src} + c0;')
+    for v in range(4):
+      self.w(f'if (c0 + {4 * v}u < {t.K}u) {{ const float4 x = *reinterpret_cast<const float4*>(p + {4 * v}); '
+             f'u[{4*v}] = x.x; u[{4*v+1}] = x.y; u[{4*v+2}] = x.z; u[{4*v+3}] = x.w; }}')
+    self.close()
+    self.w('unsigned hv[16], lv[16];')
+    self.w('#pragma unroll')
+    self.w('for (int i = 0; i < 16; ++i) { hv[i] = tfb_tc::tf32_rna(u[i]); lv[i] = __float_as_uint(u[i] - __uint_as_float(hv[i])); }')
+    self.w('tfb_tc::st_x8(slot + c0, hv);')
+    self.w(f'tfb_tc::st_x8(slot + {half}u + c0, lv);')
+    self.open(f'if (c0 + 8u < {kp}u)')
+    self.w('tfb_tc::st_x8(slot + c0 + 8u, hv + 8);')
+    self.w(f'tfb_tc::st_x8(slot + {half}u + c0 + 8u, lv + 8);')
+    self.close()
+    self.close()
+    self.w('tfb_tc::st_wait();')
+    self.w('tfb_tc::fence_before();')
+    self.w('tfb_tc::mbar_arrive(&bars[sl]);')
+    self.close()
+
+  def _producers_v3(self, s, te, tcols, NP, stage_off, lim, BAR_STAGE):
+    """Producer warps of the warp-specialised pipeline. Per tile: [barrier: abort OR] wait
+    for the stage, U pass of all terms, [barrier], loads of the next tile into the stage,
+    lane phases of the terms into the A slots. The epilogue runs on its own warps."""
+    b, H = self.base, self.H
+    pitch = self.sm['pitch']
+    nterms = len(s.terms)
+    self.open(f'else if (warp < {4 * H})')
+    self.w('const unsigned ptid = threadIdx.x;')
+    self.w('const unsigned quad = warp & 3u, grp = warp >> 2;')
+    self.w('const unsigned row = quad * 32u + lane;')
+    self.w('const unsigned lane_addr = tmem + ((quad * 32u) << 16);')
+    self.w(f'const bool lane_col = row < {tcols}u;')
+    self.w(f'const unsigned le = row / {s.N}u;')
+    self.w('unsigned it = 0;')
+    self.w('bool pending = false;')
+    self.open('if (blockIdx.x < numTiles)')
+    self._loads_v2('(size_t)blockIdx.x', 1, stage_off, BAR_STAGE, NP)
+    self._loads_v2('(size_t)blockIdx.x', 2, stage_off, BAR_STAGE, NP)
+    self.w('pending = true;')
+    self.close()
+    self.open('for (size_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++it)')
+    self.w('// every producer takes the same branches around named barriers: a timeout anywhere')
+    self.w('// stops all producers at the next tile boundary (a barrier-wide OR), never mid-tile')
+    self.w(f'if (tfb_tc::any_sync(1, {NP}, !ok)) break;')
+    self.w('const size_t ntile = tile + gridDim.x;')
+    self.w('const bool has_next = ntile < numTiles;')
+    self.w(f'if (!tfb_tc::mbar_wait(&bars[{BAR_STAGE}], it & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 40u); }}')
+    self.w('pending = false;')
+    self._u_phase_v2(stage_off, NP)
+    self.w(f'tfb_tc::named_sync(1, {NP});')
+    self.open('if (has_next)')
+    self._loads_v2('ntile', 1, stage_off, BAR_STAGE, NP)
+    self._loads_v2('ntile', 2, stage_off, BAR_STAGE, NP)
+    self.w('pending = true;')
+    self.close()
+    self.w(f'const size_t el = tile * {te}u + le;')
+    self.w('const bool active = lane_col && el < numElements && (flags == nullptr || flags[el] != 0u);')
+    for ti, t in enumerate(s.terms):
+      self._lane_v3(ti, t, lim, f'(ubuf{ti} + row * {pitch}u)', nterms)
+    self.close()
+    self.w('// a stage load still in flight after an abort must land before the CTA exits')
+    self.w(f'if (pending && !tfb_tc::mbar_wait(&bars[{BAR_STAGE}], it & 1u, {lim}ull)) atomicMax(&tfb_err_{b}, 41u);')
+    self.w('tfb_tc::cp_async_wait_all();')
+    self.w('if (ptid == 0) tfb_tc::bulk_wait();')
+    self.close()
+
+  def _epilogue_warps_v3(self, s, te, tcols, lim, n_mma):
+    """Four epilogue warps (one per TMEM lane quadrant): per tile, wait for the accumulator
+    pair, read it (main + correction), release it to the MMAs and store the lane's output
+    column straight to global memory (16-byte stores when aligned)."""
+    b = self.base
+    M = s.M
+    out = s.out
+    nld = (M + 7) // 8
+    self.open('else')
+    self.w('const unsigned equad = warp & 3u;')
+    self.w('const unsigned erow = equad * 32u + lane;')
+    self.w('const unsigned e_addr = tmem + ((equad * 32u) << 16);')
+    self.w(f'const bool ecol = erow < {tcols}u;')
+    self.w(f'const unsigned ele = erow / {s.N}u, elj = erow - ele * {s.N}u;')
+    self.w('unsigned it = 0;')
+    self.open('for (size_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++it)')
+    self.w('const unsigned db = it & 1u;')
+    self.w(f'if (!tfb_tc::mbar_wait(&bars[4u + db], (it >> 1) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 20u); break; }}')
+    self.w('tfb_tc::fence_after();')
+    self.w(f'const unsigned dm = e_addr + {self.d_base}u + db * {2 * n_mma}u;')
+    self.w(f'float acc[{nld * 8}];')
+    for k0 in range(0, nld, 2):
+      ks = list(range(k0, min(nld, k0 + 2)))
+      self.open('')
+      self.w(f'unsigned dv[{8 * len(ks)}], dc[{8 * len(ks)}];')
+      for i, k in enumerate(ks):
+        self.w(f'tfb_tc::ld_x8(dm + {8 * k}u, dv + {8 * i});')
+        self.w(f'tfb_tc::ld_x8(dm + {n_mma + 8 * k}u, dc + {8 * i});')
+      self.w('tfb_tc::ld_wait();')
+      self.w('#pragma unroll')
+      self.w(f'for (int i = 0; i < {8 * len(ks)}; ++i) acc[{8 * k0} + i] = __uint_as_float(dv[i]) + __uint_as_float(dc[i]);')
+      self.close()
+    self.w('tfb_tc::fence_before();')
+    self.w('tfb_tc::mbar_arrive(&bars[6u + db]);')
+    self.w(f'const size_t pel = tile * {te}u + ele;')
+    self.open('if (ecol && pel < numElements && (flags == nullptr || flags[pel] != 0u))')
+    self.w(f'float* const col = {self._elem_ptr(out, "pel")} + (size_t)elj * {M}u;')
+    if M % 4 == 0 and not s.accumulate:
+      self.open('if ((reinterpret_cast<uintptr_t>(col) & 15u) == 0u)')
+      self.w('#pragma unroll')
+      self.w(f'for (int i = 0; i < {M // 4}; ++i) reinterpret_cast<float4*>(col)[i] = '
+             'make_float4(acc[4 * i], acc[4 * i + 1], acc[4 * i + 2], acc[4 * i + 3]);')
+      self.close()
+      self.open('else')
+      self.w('#pragma unroll')
+      self.w(f'for (int i = 0; i < {M}; ++i) col[i] = acc[i];')
+      self.close()
+    elif s.accumulate:
+      self.w('#pragma unroll')
+      self.w(f'for (int i = 0; i < {M}; ++i) col[i] += acc[i];')
+    else:
+      self.w('#pragma unroll')
+      self.w(f'for (int i = 0; i < {M}; ++i) col[i] = acc[i];')
+    self.close()
+    self.close()
     self.close()
 
   # ------------------------------------------------------------------ producer

@@ -109,6 +109,25 @@ def test_chain_o6_bulk_and_fallback_staging(aligned):
   assert rel <= 1e-6, rel
 
 
+@pytest.mark.parametrize('n', [1, 29, 4099])
+def test_chain_o6_one_pass_pipeline(n):
+  """The one-pass producer pipeline without separate epilogue warps (plan option pipe=2,
+  the form used where the warp-specialised pipeline does not apply)."""
+  got, ref, _, _ = _run('chain_o6', 'tf32x3', n, variant={'pipe': 2})
+  rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+  assert rel <= 1e-6, rel
+
+
+@pytest.mark.parametrize('case,n', [('chain_o4_q27', 1), ('chain_o4_q27', 77), ('chain_o4_q27', 1001)])
+def test_warp_specialised_pipeline_other_shape(case, n):
+  """27 quantities: 4 elements per tile, 24-column A slots, 32-column accumulators."""
+  g = __import__('tensorforge_b200.kernels', fromlist=['make']).make(case, 'float', precision='tf32x3')
+  assert g.get_plan().params['pipe'] == 3
+  got, ref, _, _ = _run(case, 'tf32x3', n)
+  rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+  assert rel <= 1e-6, rel
+
+
 @pytest.mark.parametrize('precision', ['tf32x3', 'bf16x3'])
 def test_chain_o6_per_term_pipeline(precision):
   """The per-term producer pipeline (plan option pipe=1), kept for shapes whose buffers

@@ -13,7 +13,16 @@ def _shape(case):
 
 def test_default_is_form_u():
   p = make('chain_o6', 'float', precision='tf32x3').get_plan()
-  assert p.strategy == 'tcsplit' and 'form' not in p.params and p.params['pipe'] == 2
+  assert p.strategy == 'tcsplit' and 'form' not in p.params and p.params['pipe'] == 3
+
+
+def test_warp_specialised_pipeline_eligibility():
+  """pipe 3 (separate epilogue warps, two A slots, two accumulator pairs) needs TF32
+  splits, a U pass per term with K a multiple of 4, and TMEM for 2 slots + 2 pairs."""
+  assert make('chain_o4_q27', 'float', precision='tf32x3').get_plan().params['pipe'] == 3
+  assert make('chain_o6', 'float', precision='bf16x3').get_plan().params['pipe'] == 2
+  assert make('chain_o3_dense', 'float', precision='tf32x3').get_plan().params['pipe'] == 2   # K = 10
+  assert make('chain_o6', 'float', precision='tf32x3', variant={'pipe': 2}).get_plan().params['pipe'] == 2
 
 
 @pytest.mark.parametrize('acc,bbuf', [(1, 1), (1, 2), (2, 1), (2, 2)])
