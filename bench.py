@@ -454,6 +454,16 @@ def extra_workloads(stream, short=False, cpu=True):
                                          'peak_source': 'FP32: FFMA probe of this run; HBM: measured copy bandwidth'}}
   if cpu:
     out['c3_mixed_shapes']['cpu_baseline'] = reference_cpu_mixed(groups)
+  # config 4: the shipped cost model on held-out chains of the seeded tuning set, every
+  # variant re-measured here (the exhaustive tuner's timings), bounded in time
+  from tensorforge_b200.tune import heldout, select
+  t4 = time.time()
+  recs = heldout.measure_all(heldout.build_all(heldout.heldout_specs(40)), time_limit=20 if short else 60)
+  c4 = heldout.summary(heldout.score(recs, select.predict))
+  c4.update({'chains_requested': 40, 'seconds': time.time() - t4, 'inference': select.last_inference,
+             'regret': '(measured time of pick - measured best) / measured best; default = the planner '
+                       'without the cost model; chains from the 20 % test split of the 2,000-chain set'})
+  out['c4_cost_model'] = c4
   # config 2: log-uniform magnitudes through every precision variant, error vs the FP64 oracle
   descrs = cases.build(CASE, cases.ns_from_module('tensorforge_b200'))
   n2 = 100000 if short else 500000
@@ -555,9 +565,11 @@ def impl_ours(args, rank, world, dist):
   device = torch.device('cuda', torch.cuda.current_device())
   n = args.elements
   variants = ['plain'] if args.variant == 'plain' else (
-    [args.variant] if args.variant != 'auto' else ['tf32x3', 'plain', 'tf32x3_form_b', 'tf32x3_form_b2', 'tf32x3_form_b_ws'])
+    [args.variant] if args.variant != 'auto' else ['tf32x3', 'plain', 'tf32x3_pipe2', 'tf32x3_form_b', 'tf32x3_form_b2',
+                                                   'tf32x3_form_b_ws'])
   opts_of = {'plain': {}, 'tf32x3': {'precision': 'tf32x3'},
              'tf32x3_ahead': {'precision': 'tf32x3', 'variant': {'form': 'u', 'ahead': 1}},
+             'tf32x3_pipe2': {'precision': 'tf32x3', 'variant': {'form': 'u', 'pipe': 2}},
              'tf32x3_form_b': {'precision': 'tf32x3', 'variant': {'form': 'b'}},
              'tf32x3_form_b2': {'precision': 'tf32x3', 'variant': {'form': 'b', 'bbuf': 2}},
              'tf32x3_form_b_ws': {'precision': 'tf32x3', 'variant': {'form': 'b', 'ws': 1}},

@@ -305,11 +305,17 @@ class GenericEmitter:
         else:
           self.w(f'{const}{T}* const glb_{o.name} = active ? {o.name}[batchId] + {o.name}_extraOffset : nullptr;')
       first_use = live_ranges(chain)
+      access = [_stage_access(st) for st in chain.stages]
+      shared_first = {}
+      for o in chain.operands:
+        if o.kind == 'shared' and o.sparse:
+          used = [i for i, (_, r) in enumerate(access) if id(o) in r]
+          shared_first[o.name] = min(used) if used else 0
       for si, st in enumerate(chain.stages):
         # batched sparse operands are expanded right before the first stage that reads them
         # (their region may reuse the memory of regions that are dead by then)
         shared_now = [o for o in chain.operands if o.kind == 'shared' and o.sparse and o.name not in self.resident
-                      and min([i for i, (_, r) in enumerate(map(_stage_access, chain.stages)) if id(o) in r] + [0]) == si]
+                      and shared_first[o.name] == si]
         if shared_now:
           self.w('__syncthreads();  // every element group is done with the region\'s previous operand')
           for o in shared_now:

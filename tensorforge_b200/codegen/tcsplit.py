@@ -197,7 +197,8 @@ def plan(chain, shape, precision, variant):
   for t in shape.terms:
     if t.R is not None and t.R.kind != 'batched':
       return None
-  pipe = variant.get('pipe', 3 if pipe3_ok(shape, precision, variant.get('chunk', 16)) else 2)
+  default_pipe = 3 if (pipe3_ok(shape, precision, variant.get('chunk', 16)) and not variant.get('ahead')) else 2
+  pipe = variant.get('pipe', default_pipe)
   if pipe == 3 and not pipe3_ok(shape, precision, variant.get('chunk', 16)):
     pipe = 2
   sm = smem_plan_v2(shape, precision) if pipe in (2, 3) else None

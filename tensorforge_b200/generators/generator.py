@@ -211,11 +211,14 @@ class Generator:
   def _tuned_variant(self):
     """Variant picked by Options.tuner ('model' / 'exhaustive'), None for the planner's own.
 
-    Only plain-precision chains without an explicit variant are tuned; the cost model was
-    trained on FP32 timings, so FP64 chains keep the planner's choice under 'model'.
+    Chains without an explicit variant are tuned: plain-precision ones by either tuner
+    (the cost model was trained on FP32 timings, so FP64 chains keep the planner's choice
+    under 'model'), TF32x3 ones by the exhaustive tuner over the tensor-core variants.
     """
     opts = self._context.get_user_options()
-    if opts.tuner == 'heuristic' or opts.variant or opts.precision != 'plain':
+    if opts.tuner == 'heuristic' or opts.variant:
+      return None
+    if opts.precision != 'plain' and not (opts.tuner == 'exhaustive' and opts.precision == 'tf32x3'):
       return None
     from ..tune import select
     if opts.tuner == 'model':

@@ -1,14 +1,18 @@
 """Variant selection at generation time: `Options(tuner='model')` and `tuner='exhaustive'`.
 
 'model'       ranks every applicable variant with the trained cost model (weights shipped
-              in model_b200.npz, trained on B200 timings; evaluated on the host, no GPU
-              needed) and takes the best predicted one.
+              in model_b200.npz, trained on B200 timings) and takes the best predicted
+              one. The network runs on the GPU through the native MLP kernels
+              (tfb_mlp_forward) when a CUDA device is present; generation on a machine
+              without one evaluates the same network on the host.
 'exhaustive'  builds every variant and times it on the current GPU (CUDA events, best of
               3) with synthetic inputs of `batch` elements, and takes the fastest.
 
-Both only choose among variants of the plain-precision generators (generic and column
-programs); the tensor-core precisions have one plan each. Launchers are generic in
-numElements, so the batch the choice is made for is a parameter (default 100,000).
+'model' chooses among the plain-precision variants it was trained on (generic lane
+groups and elements per CTA, column programs). 'exhaustive' also times the points per
+lane of elementwise stages and, for precision 'tf32x3', the tensor-core variants
+(operand forms U and B, producer pipelines). Launchers are generic in numElements, so
+the batch the choice is made for is a parameter (default 100,000).
 """
 import os
 
@@ -31,14 +35,47 @@ def _load_model():
   return _model
 
 
+_gpu_model = None
+last_inference = None   # 'gpu' or 'host': where the latest model_choice ran the network
+
+
+def _device_model():
+  """The shipped weights in a CostModel on the GPU (native MLP kernels), or None when no
+  CUDA device (or no native runtime library) is available."""
+  global _gpu_model
+  if _gpu_model is None:
+    try:
+      import torch
+      if not torch.cuda.is_available():
+        return None
+      from .cost_model import CostModel
+      m = CostModel()
+      m.load(MODEL_PATH)
+      _gpu_model = m
+    except (ImportError, OSError, RuntimeError):
+      return None
+  return _gpu_model
+
+
+def predict(feats):
+  """Predicted log-runtimes of feature rows: on the GPU when possible, else on the host."""
+  global last_inference
+  m = _device_model()
+  if m is not None:
+    last_inference = 'gpu'
+    return m.predict(feats)
+  from .cost_model import host_predict
+  params, mean, std = _load_model()
+  last_inference = 'host'
+  return host_predict(params, mean, std, feats)
+
+
 def model_choice(chain, fp_size=4, batch=DEFAULT_BATCH):
   """Variant dict with the lowest predicted runtime, or None if there is no choice."""
-  from .cost_model import host_predict
-  cands = variant_space(chain, fp_size)
+  cands = variant_space(chain, fp_size, model_only=True)
   if len(cands) < 2:
     return None
-  params, mean, std = _load_model()
-  pred = host_predict(params, mean, std, [features(chain, v, batch) for v in cands])
+  pred = predict([features(chain, v, batch) for v in cands])
   return cands[int(np.argmin(pred))]
 
 
@@ -58,7 +95,7 @@ def exhaustive_choice(descr_list, context, batch=DEFAULT_BATCH, reps=3):
     return g
 
   base = gen(None)
-  cands = variant_space(base.get_chain(), context.fp_type.size())
+  cands = variant_space(base.get_chain(), context.fp_type.size(), opts.precision)
   if len(cands) < 2:
     return None
   dtype = torch.float64 if context.fp_type.size() == 8 else torch.float32

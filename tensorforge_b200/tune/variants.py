@@ -7,22 +7,55 @@ from ..plan.chains import match_left_chain
 GENERIC_G = (4, 8, 16, 32, 64, 128, 256)
 GENERIC_E = (1, 2, 4, 8, 16)
 COLPROG = [dict(threads=t, a_source=a) for t in (128, 256) for a in ("const", "smem")]
+# points each lane evaluates per pass in elementwise stages (generic generator)
+POINTS_PER_LANE = (1, 2, 4, 8)
+# tensor-core (TF32x3) variants: operand form U with the warp-specialised (3) or one-pass (2)
+# producer pipeline, operand form B with one or two B buffers
+TCSPLIT = [{'strategy': 'tcsplit', 'form': 'u', 'pipe': 3}, {'strategy': 'tcsplit', 'form': 'u', 'pipe': 2},
+           {'strategy': 'tcsplit', 'form': 'b', 'bbuf': 1}, {'strategy': 'tcsplit', 'form': 'b', 'bbuf': 2}]
 NFEAT = 32
 TUNE_COLPROG_MAX_FMAS = 2048
 
 
-def variant_space(chain, fp_size=4):
-  """Variant dicts (Options.variant) that apply to `chain`."""
+def tensor_core_space(chain, precision='tf32x3'):
+  """Tensor-core variants that the planner realises for `chain` (distinct plans only)."""
+  from ..plan.chains import tcsplit_plan
+  shape = match_left_chain(chain)
+  if shape is None:
+    return []
+  out, seen = [], set()
+  for v in TCSPLIT:
+    p = tcsplit_plan(chain, shape, precision, v)
+    if p is None or p.key() in seen:
+      continue
+    seen.add(p.key())
+    out.append(dict(v))
+  return out
+
+
+def variant_space(chain, fp_size=4, precision='plain', model_only=False):
+  """Variant dicts (Options.variant) that apply to `chain`.
+
+  precision 'tf32x3': the tensor-core variants (timed by the exhaustive tuner). For plain
+  chains with elementwise stages the generic variants also vary the points per lane,
+  except with `model_only` (the cost model was trained on the default of 4)."""
   from ..codegen.generic import smem_layout
+  if precision == 'tf32x3':
+    return tensor_core_space(chain, precision)
   out = []
   shared, per_elem = smem_layout(chain)
+  ppl = (None,) if (model_only or not chain.has_elementwise()) else POINTS_PER_LANE
   for g in GENERIC_G:
     for e in GENERIC_E:
       if g * e > 1024 or g * e < 32:
         continue
       if (shared + per_elem * e) * fp_size > SMEM_LIMIT:
         continue
-      out.append({'strategy': 'generic', 'threads_per_element': g, 'elements_per_block': e})
+      for u in ppl:
+        v = {'strategy': 'generic', 'threads_per_element': g, 'elements_per_block': e}
+        if u is not None:
+          v['points_per_lane'] = u
+        out.append(v)
   shape = match_left_chain(chain)
   if shape is not None and shape.M <= 128 and shape.N <= 128:
     # tuning builds every variant; column programs with large A cost ptxas close to a
@@ -74,8 +107,9 @@ def variant_features(chain, variant, fp_size=4):
   if variant['strategy'] == 'generic':
     g, e = variant['threads_per_element'], variant['elements_per_block']
     smem = (shared + per_elem * e) * fp_size
+    ppl = variant.get('points_per_lane', 4) if chain.has_elementwise() else 0
     return [1.0, 0.0, _l2(g) / 6.0, _l2(e) / 4.0, g * e / 1024.0, 0.0, 0.0, smem / SMEM_LIMIT,
-            math.log10(max(1, per_elem * fp_size)) / 5.0, 0.0, 0.0, 0.0]
+            math.log10(max(1, per_elem * fp_size)) / 5.0, 0.0, 0.0, ppl / 8.0 if ppl != 4 else 0.0]
   t = variant['threads']
   shape = match_left_chain(chain)
   te = max(1, t // shape.N)
@@ -101,5 +135,5 @@ def effective_variant(plan):
 def space_signature():
   """Short hash of the variant space: tuning results are only comparable within one space."""
   import hashlib
-  key = repr((GENERIC_G, GENERIC_E, COLPROG, TUNE_COLPROG_MAX_FMAS, NFEAT))
+  key = repr((GENERIC_G, GENERIC_E, COLPROG, TUNE_COLPROG_MAX_FMAS, NFEAT))  # the timed plain space
   return hashlib.sha1(key.encode()).hexdigest()[:8]

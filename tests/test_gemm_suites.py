@@ -78,3 +78,32 @@ def test_suite_case_generates_and_oracle_matches_numpy(case):
           bv = B(j, k) if case['trans_b'] else B(k, j)
           acc += a * bv
         assert abs(C(i, j) - case['alpha'] * acc) <= 1e-12 * (1 + abs(acc))
+
+
+BEHAVIOUR = json.load(open(os.path.join(HERE, 'golden', 'suite_reference_behaviour.json')))
+
+
+@pytest.mark.parametrize('case', SUITES, ids=[c['id'] for c in SUITES])
+def test_rejected_case_has_a_recorded_reference_behaviour(case):
+  """Every suite case this generator rejects is one the reference cannot serve either
+  (tests/golden/make_suite_reference.py ran the reference generator on each): it does not
+  generate (NameError on transposes), or its kernel writes outside the destination's
+  bounding box or outside the element's data (or the host process dies)."""
+  from tensorforge_b200.common.context import Context, Options
+  from tensorforge_b200.common.basic_types import FloatingPointType
+  from tensorforge_b200.common.exceptions import GenerationError
+  from tensorforge_b200.generators.generator import Generator
+  g = Generator(_build(case), Context('sm_100a', 'cuda', FloatingPointType.FLOAT, Options()))
+  try:
+    g.generate()
+    assert case['id'] not in BEHAVIOUR
+    return
+  except GenerationError:
+    pass
+  rec = BEHAVIOUR[case['id']]
+  if not rec['generates']:
+    assert 'Error' in rec['error']
+  elif 'error' in rec:
+    assert 'died' in rec['error'] or 'timed out' in rec['error']
+  else:
+    assert rec['outside_box'] > 0 or rec['outside_data'] > 0
