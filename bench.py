@@ -570,6 +570,7 @@ def impl_ours(args, rank, world, dist):
   opts_of = {'plain': {}, 'tf32x3': {'precision': 'tf32x3'},
              'tf32x3_ahead': {'precision': 'tf32x3', 'variant': {'form': 'u', 'ahead': 1}},
              'tf32x3_pipe2': {'precision': 'tf32x3', 'variant': {'form': 'u', 'pipe': 2}},
+             'plain_rs2': {'variant': {'strategy': 'colprog', 'threads': 256, 'rsplit': 2, 'min_blocks': 2}},
              'tf32x3_form_b': {'precision': 'tf32x3', 'variant': {'form': 'b'}},
              'tf32x3_form_b2': {'precision': 'tf32x3', 'variant': {'form': 'b', 'bbuf': 2}},
              'tf32x3_form_b_ws': {'precision': 'tf32x3', 'variant': {'form': 'b', 'ws': 1}},
@@ -588,7 +589,7 @@ def impl_ours(args, rank, world, dist):
     except Exception as e:  # variant not available for this chain
       log(f'variant {name} unavailable: {e}')
       continue
-    if name != 'plain' and gen.get_plan().strategy == 'colprog':
+    if name.startswith(('tf32x3', 'bf16x3')) and gen.get_plan().strategy != 'tcsplit':
       log(f'variant {name} fell back to {gen.get_plan().strategy}; skipped')
       continue
     k = compile_generator(gen)

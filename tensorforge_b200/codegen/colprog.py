@@ -80,9 +80,14 @@ class _ColProg:
     self.term_const = [ti < self.const_terms for ti in range(nterms)]
     self.prefetch = bool(plan.params.get('prefetch', 1)) and not getattr(self, 'grouped', False)
     self.CPT = int(plan.params.get('cols', 1))
-    self.TE = tile_elements(shape, self.BT, self.CPT)
+    # row split: RS groups of threads share the tile's columns, group g accumulating rows
+    # [g * MR, (g + 1) * MR) of every column it owns (RS x the warps for the same registers)
+    self.RS = int(plan.params.get('rsplit', 1))
+    self.CT = self.BT // self.RS          # threads per row group (column threads)
+    self.TE = tile_elements(shape, self.CT, self.CPT)
     self.TC = self.TE * shape.N
     self.TCT = self.TC // self.CPT        # columns per round: thread t owns t + r * TCT
+    self.MR = _pad(-(-shape.M // self.RS), self.VEC) if self.RS > 1 else shape.M
     self.kmax = max(t.K for t in shape.terms)
     # U^T rows: K + VEC values keep 16-byte row starts (vector loads) and spread the rows of
     # a quarter-warp over the banks; an odd pitch (scalar loads) is conflict-free and smaller
@@ -241,12 +246,16 @@ class _ColProg:
   def _tile_body(self):
     """Code for one tile; expects `tile`, `ubuf`, (`sA`), the ABI names, numElements, flags."""
     s, T, BT = self.s, self.T, self.BT
-    self.w(f'const unsigned le = threadIdx.x / {s.N}u, lj = threadIdx.x - le * {s.N}u;')
+    if self.RS > 1:
+      self.w(f'const unsigned ct = threadIdx.x % {self.CT}u, rg = threadIdx.x / {self.CT}u;')
+    else:
+      self.w('const unsigned ct = threadIdx.x;')
+    self.w(f'const unsigned le = ct / {s.N}u, lj = ct - le * {s.N}u;')
     self.w(f'const size_t e0 = tile * {self.TE}u;')
     for r in range(self.CPT):
       sfx = '' if r == 0 else str(r)
       self.w(f'const size_t el{sfx} = e0 + le + {r * (self.TCT // s.N)}u;')
-      self.w(f'const bool lane_ok{sfx} = threadIdx.x < {self.TCT}u && el{sfx} < numElements;')
+      self.w(f'const bool lane_ok{sfx} = ct < {self.TCT}u && el{sfx} < numElements;')
       self.w(f'const bool active{sfx} = lane_ok{sfx} && (flags == nullptr || flags[el{sfx}] != 0u);')
     for name, off in ([] if self.prefetch else self.r_off.items()):
       op = [o for o in self.chain.operands if o.name == name][0]
@@ -261,9 +270,9 @@ class _ColProg:
       self.w('__syncthreads();')
     for r in range(self.CPT):
       a = 'acc' if r == 0 else f'acc{r}'
-      self.w(f'{T} {a}[{s.M}];')
+      self.w(f'{T} {a}[{self.MR}];')
       self.w('#pragma unroll')
-      self.w(f'for (int i = 0; i < {s.M}; ++i) {a}[i] = {self.lit(0)};')
+      self.w(f'for (int i = 0; i < {self.MR}; ++i) {a}[i] = {self.lit(0)};')
     for ti, t in enumerate(s.terms):
       self._term(ti, t)
     self._epilogue()
@@ -467,9 +476,26 @@ class _ColProg:
     sfx = lambda r: '' if r == 0 else str(r)
     self.open('if (' + ' || '.join(f'active{sfx(r)}' for r in R) + ')')
     for r in R:
-      self.w(f'const {T}* const ucol{sfx(r)} = ubuf + (threadIdx.x + {r * self.TCT}u) * {pitch}u;')
+      self.w(f'const {T}* const ucol{sfx(r)} = ubuf + (ct + {r * self.TCT}u) * {pitch}u;')
     cols = a_values(t)
     comps = ['x', 'y', 'z', 'w'][:VEC]
+    for g in range(self.RS):
+      r0, r1 = g * self.MR, min(s.M, (g + 1) * self.MR)
+      if self.RS > 1:
+        self.open(f'if (rg == {g}u)')
+      self._k_stage_rows(ti, t, cols, r0, r1, comps)
+      if self.RS > 1:
+        self.close()
+    self.close()
+    self.w('__syncthreads();')
+
+  def _k_stage_rows(self, ti, t, cols, r0, r1, comps):
+    """Unrolled FMAs of term ti over the nonzeros of A_t in rows [r0, r1) (acc index i - r0)."""
+    T, VEC, VT, FMA, LC = self.T, self.VEC, self.VT, self.FMA, self.LC
+    b = self.base
+    K = t.K
+    R = range(self.CPT)
+    sfx = lambda r: '' if r == 0 else str(r)
     # shared-memory A is consumed in storage order: fetch it one aligned vector at a time
     # (one broadcast LDS.128 / LDS.64 per VEC values) instead of one load per value
     loaded = set()
@@ -485,6 +511,8 @@ class _ColProg:
       return f'av{v}.{comps[g % VEC]}'
     for l0 in range(0, K, LC):
       n = min(LC, K - l0)
+      if not any(r0 <= i < r1 for l in range(l0, l0 + n) for (i, _) in cols[l][1]):
+        continue
       self.open('')
       loaded.clear()  # vectors are declared per chunk block
       for r in R:
@@ -498,19 +526,19 @@ class _ColProg:
           self.w(f'{u}[{i}] = {uc}[{l0 + i}];')
       for l in range(l0, l0 + n):
         for (i, pos) in cols[l][1]:
+          if not r0 <= i < r1:
+            continue
           a = a_operand(pos)
           if self.CPT == 1:
-            self.w(f'acc[{i}] = {FMA}({a}, u[{l - l0}], acc[{i}]);')
+            self.w(f'acc[{i - r0}] = {FMA}({a}, u[{l - l0}], acc[{i - r0}]);')
           else:
             self.open('')
             self.w(f'const {T} av = {a};')
             for r in R:
               acc = f'acc{sfx(r)}'
-              self.w(f'{acc}[{i}] = {FMA}(av, u{sfx(r)}[{l - l0}], {acc}[{i}]);')
+              self.w(f'{acc}[{i - r0}] = {FMA}(av, u{sfx(r)}[{l - l0}], {acc}[{i - r0}]);')
             self.close()
       self.close()
-    self.close()
-    self.w('__syncthreads();')
 
   def _epilogue(self):
     """Elementwise stages on the finished output column in registers (row i = n0, the
@@ -549,14 +577,26 @@ class _ColProg:
     sfx = lambda r: '' if r == 0 else str(r)
     coalesced = (o.addressing.name == 'STRIDED' and vol == M * s.N and vol % VEC == 0 and M % VEC == 0
                  and not s.accumulate)
+    groups = [(g, g * self.MR, min(M, (g + 1) * self.MR)) for g in range(self.RS)]
+
+    def by_group(body):
+      for g, r0, r1 in groups:
+        if self.RS > 1:
+          self.open(f'if (rg == {g}u)')
+        body(r0, r1)
+        if self.RS > 1:
+          self.close()
 
     def per_column():
       for r in range(self.CPT):
         self.open(f'if (active{sfx(r)})')
         self.w(f'{T}* const col = {self._elem_ptr(o, "el" + sfx(r))} + (size_t)lj * {M}u;')
-        self.w('#pragma unroll')
         op = '+=' if s.accumulate and not s.epilogue else '='
-        self.w(f'for (int i = 0; i < {M}; ++i) col[i] {op} acc{sfx(r)}[i];')
+
+        def body(r0, r1, r=r):
+          self.w('#pragma unroll')
+          self.w(f'for (int i = {r0}; i < {r1}; ++i) col[i] {op} acc{sfx(r)}[i - {r0}];')
+        by_group(body)
         self.close()
 
     if coalesced:
@@ -566,9 +606,12 @@ class _ColProg:
       self.open('if (vec_out)')
       for r in range(self.CPT):
         self.open(f'if (lane_ok{sfx(r)})')
-        for v in range(M // VEC):
-          vals = ', '.join(f'acc{sfx(r)}[{v * VEC + c}]' for c in range(VEC))
-          self.w(f'reinterpret_cast<{VT}*>(ubuf + (threadIdx.x + {r * self.TCT}u) * {M}u)[{v}] = make_{VT}({vals});')
+
+        def body(r0, r1, r=r):
+          for v in range(r0 // VEC, r1 // VEC):
+            vals = ', '.join(f'acc{sfx(r)}[{v * VEC + c - r0}]' for c in range(VEC))
+            self.w(f'reinterpret_cast<{VT}*>(ubuf + (ct + {r * self.TCT}u) * {M}u)[{v}] = make_{VT}({vals});')
+        by_group(body)
         self.close()
       self.w('__syncthreads();')
       self.w(f'const size_t nvalid = (numElements - e0) < {self.TE}u ? (numElements - e0) : {self.TE}u;')

@@ -146,6 +146,27 @@ def smem_plan_v2(shape, precision):
               pitch=pitch, ubuf_bytes=ubuf, off_bar=off_bar, total=total, te=te, tc=tc)
 
 
+def smem_plan_v3(shape, precision):
+  """Shared memory of the warp-specialised pipeline: the one-pass layout with the B operand
+  stored for the real output rows only (rows M..N_mma-1 of the MMA's B tile then read the
+  next block, and land in accumulator columns the epilogue never reads) and, when it fits,
+  an output staging buffer for the epilogue warps' bulk stores."""
+  sm = smem_plan_v2(shape, precision)
+  lay = layout(shape, precision)
+  rows_b = _pad(shape.M, 8)
+  b_bytes = sum(2 * rows_b * kp * lay['es'] for kp in lay['kpad'])
+  shift = sm['off_stage'] - _pad(b_bytes, 128)
+  out = dict(sm, rows_b=rows_b, b_bytes=b_bytes)
+  for k in ('off_stage', 'off_u', 'off_bar', 'total'):
+    out[k] = sm[k] - shift
+  ost = _pad(sm['tc'] * shape.M * 4, 128)
+  if shape.M % 4 == 0 and out['total'] + ost <= _plan.SMEM_LIMIT:
+    out['off_ost'] = out['off_bar']
+    out['off_bar'] += ost
+    out['total'] += ost
+  return out
+
+
 def pipe3_ok(shape, precision, chunk=16):
   """The warp-specialised pipeline (pipe 3) needs TF32 splits, a U pass for every term
   (K a multiple of 4, lane phases of at most 4 x 16 columns) and tensor memory for two A
@@ -201,7 +222,7 @@ def plan(chain, shape, precision, variant):
   pipe = variant.get('pipe', default_pipe)
   if pipe == 3 and not pipe3_ok(shape, precision, variant.get('chunk', 16)):
     pipe = 2
-  sm = smem_plan_v2(shape, precision) if pipe in (2, 3) else None
+  sm = (smem_plan_v3 if pipe == 3 else smem_plan_v2)(shape, precision) if pipe in (2, 3) else None
   if sm is None or sm['total'] > _plan.SMEM_LIMIT:
     pipe = 1
     sm = smem_plan(shape, precision)
@@ -212,6 +233,8 @@ def plan(chain, shape, precision, variant):
   params = {'precision': precision, 'chunk': chunk, 'pipe': pipe}
   if int(variant.get('ahead', 0)) and pipe == 2:
     params['ahead'] = 1
+  if int(variant.get('urows', 1)) == 2 and pipe in (2, 3) and all(t.K % 2 == 0 for t in shape.terms):
+    params['urows'] = 2
   if int(variant.get('wait_probe', 0)) > 0:
     # failure-detection check: the kernel first waits, with this many polls, on an mbarrier
     # that nothing arrives on, records error 30 and returns before issuing any copy or MMA
@@ -360,7 +383,8 @@ class _TC:
     self.prec = plan_.params['precision']
     self.lay = layout(shape, self.prec)
     self.pipe = plan_.params.get('pipe', 1)
-    self.sm = smem_plan_v2(shape, self.prec) if self.pipe in (2, 3) else smem_plan(shape, self.prec)
+    self.sm = ({3: smem_plan_v3, 2: smem_plan_v2}[self.pipe](shape, self.prec) if self.pipe in (2, 3)
+               else smem_plan(shape, self.prec))
     self.LC = plan_.params['chunk']
     self.ahead = bool(plan_.params.get('ahead', 0))
     self.H = H_GROUPS
@@ -423,15 +447,17 @@ class _TC:
     ke = 16 // es
     b_off = []
     off = 0
+    rows_b = sm.get('rows_b', n_mma)   # B rows stored (the MMA's N tile reads n_mma)
+    self.rows_b = rows_b
     for kp in lay['kpad']:
-      b_off.append((off, off + n_mma * kp * es))
-      off += 2 * n_mma * kp * es
+      b_off.append((off, off + rows_b * kp * es))
+      off += 2 * rows_b * kp * es
     gathers = []
     for ti, t in enumerate(s.terms):
       kp = lay['kpad'][ti]
       look = t.A.sparse_lookup() if t.A.sparse else None
       tbl = []
-      for n in range(n_mma):
+      for n in range(rows_b):
         for k in range(kp):
           if n < t.A.shape[0] and k < t.K:
             tbl.append(k * t.A.shape[0] + n if look is None else look.get((n, k), -1))
@@ -505,7 +531,7 @@ class _TC:
       kp = lay['kpad'][ti]
       hi_off, lo_off = b_off[ti]
       sbo = (kp // ke) * 128
-      self.open(f'for (int q = threadIdx.x; q < {n_mma * kp}; q += blockDim.x)')
+      self.open(f'for (int q = threadIdx.x; q < {rows_b * kp}; q += blockDim.x)')
       self.w(f'const int n = q / {kp}, k = q - n * {kp};')
       self.w(f'const int src = bgather{ti}_{b}[q];')
       self.w(f'const float v = src >= 0 ? {t.A.name}[src] : 0.0f;')
@@ -791,24 +817,38 @@ class _TC:
 
   def _u_phase_v2(self, stage_off, NP):
     """U_t = B * R_t for every term in one pass: one thread per (element, row l) loads row l
-    of B once and writes row l of every U_t that uses it (R_t's pattern unrolled)."""
+    of B once and writes row l of every U_t that uses it (R_t's pattern unrolled). With plan
+    option `urows=2` a thread takes rows l and l + 1 (64-bit loads and stores, R's values
+    loaded once for both)."""
     s, sm = self.s, self.sm
     te, pitch, N = sm['te'], sm['pitch'], s.N
     comp = ['x', 'y', 'z', 'w']
+    two = int(self.plan.params.get('urows', 1)) == 2
     for B in sm['b_ops']:
       terms = [(ti, t) for ti, t in enumerate(s.terms) if t.B is B]
       K, P = terms[0][1].K, terms[0][1].P
       bvals = _pad(B.element_volume(), 4)
-      self.open(f'for (unsigned q = ptid; q < {te * K}u; q += {NP}u)')
-      self.w(f'const unsigned ei = q / {K}u, l = q - ei * {K}u;')
-      self.w(f'const float* const bq = stage + {stage_off[B.name]} + ei * {bvals}u + l;')
-      for m in range(P):
-        self.w(f'const float q{m} = bq[{m * K}];')
+      if two:
+        assert K % 2 == 0 and pitch % 2 == 0 and stage_off[B.name] % 2 == 0
+        self.open(f'for (unsigned q = ptid; q < {te * K // 2}u; q += {NP}u)')
+        self.w(f'const unsigned ei = q / {K // 2}u, l = 2u * (q - ei * {K // 2}u);')
+        self.w(f'const float* const bq = stage + {stage_off[B.name]} + ei * {bvals}u + l;')
+        for m in range(P):
+          self.w(f'const float2 q{m} = *reinterpret_cast<const float2*>(bq + {m * K});')
+      else:
+        self.open(f'for (unsigned q = ptid; q < {te * K}u; q += {NP}u)')
+        self.w(f'const unsigned ei = q / {K}u, l = q - ei * {K}u;')
+        self.w(f'const float* const bq = stage + {stage_off[B.name]} + ei * {bvals}u + l;')
+        for m in range(P):
+          self.w(f'const float q{m} = bq[{m * K}];')
       for ti, t in terms:
         dst = f'ubuf{ti}[(ei * {N}u + {{j}}u) * {pitch}u + l]'
         if t.R is None:
           for j in range(N):
-            self.w(f'{dst.format(j=j)} = q{j};')
+            if two:
+              self.w(f'*reinterpret_cast<float2*>(&{dst.format(j=j)}) = q{j};')
+            else:
+              self.w(f'{dst.format(j=j)} = q{j};')
           continue
         nr = t.R.storage_size()
         self.open('')
@@ -817,12 +857,20 @@ class _TC:
           self.w(f'const float4 r{v} = rq[{v}];')
         look = t.R.sparse_lookup() if t.R.sparse else None
         for j in range(N):
-          expr = '0.0f'
+          ex, ey = '0.0f', '0.0f'
           for m in range(P):
             pos = look.get((m, j)) if look is not None else j * P + m
             if pos is not None:
-              expr = f'fmaf(q{m}, r{pos // 4}.{comp[pos % 4]}, {expr})'
-          self.w(f'{dst.format(j=j)} = {expr};')
+              r = f'r{pos // 4}.{comp[pos % 4]}'
+              if two:
+                ex = f'fmaf(q{m}.x, {r}, {ex})'
+                ey = f'fmaf(q{m}.y, {r}, {ey})'
+              else:
+                ex = f'fmaf(q{m}, {r}, {ex})'
+          if two:
+            self.w(f'*reinterpret_cast<float2*>(&{dst.format(j=j)}) = make_float2({ex}, {ey});')
+          else:
+            self.w(f'{dst.format(j=j)} = {ex};')
         self.close()
       self.close()
 
@@ -1059,7 +1107,35 @@ class _TC:
     self.w('tfb_tc::fence_before();')
     self.w('tfb_tc::mbar_arrive(&bars[6u + db]);')
     self.w(f'const size_t pel = tile * {te}u + ele;')
-    self.open('if (ecol && pel < numElements && (flags == nullptr || flags[pel] != 0u))')
+    staged = ('off_ost' in self.sm and out.addressing.name == 'STRIDED' and not s.accumulate
+              and out.element_volume() == M * s.N and M % 4 == 0)
+    if staged:
+      # the warp's 32 rows are 32 consecutive output columns of the tile: stage them in
+      # shared memory and write them with one bulk copy (unmasked, 16-byte aligned output)
+      vol = out.element_volume()
+      self.w(f'float* const obase = {out.name} + tile * {te * vol}u + {out.name}_extraOffset;')
+      self.open('if (flags == nullptr && (reinterpret_cast<uintptr_t>(obase) & 15u) == 0u)')
+      self.w(f'float* const ost = reinterpret_cast<float*>(tfb_smem_raw + {self.sm["off_ost"]});')
+      self.w('if (lane == 0 && it > 0) tfb_tc::bulk_wait_read();  // the previous tile\'s copy has read the buffer')
+      self.w('__syncwarp();')
+      self.w('// rows past the tile\'s columns have no place in the buffer')
+      self.open('if (ecol)')
+      self.w('#pragma unroll')
+      self.w(f'for (int i = 0; i < {M // 4}; ++i) reinterpret_cast<float4*>(ost + erow * {M}u)[i] = '
+             'make_float4(acc[4 * i], acc[4 * i + 1], acc[4 * i + 2], acc[4 * i + 3]);')
+      self.close()
+      self.w('tfb_tc::fence_proxy_async();')
+      self.w('__syncwarp();')
+      self.open('if (lane == 0)')
+      self.w(f'const size_t nrows = (numElements - tile * {te}u) < {te}u ? (numElements - tile * {te}u) * {s.N}u : {te * s.N}u;')
+      self.w('const size_t r0 = equad * 32u;')
+      self.w('const unsigned rows = nrows > r0 ? (unsigned)(nrows - r0 < 32u ? nrows - r0 : 32u) : 0u;')
+      self.w(f'if (rows > 0u) tfb_tc::bulk_store(obase + r0 * {M}u, ost + r0 * {M}u, rows * {M * 4}u);')
+      self.close()
+      self.close()
+      self.open('else if (ecol && pel < numElements && (flags == nullptr || flags[pel] != 0u))')
+    else:
+      self.open('if (ecol && pel < numElements && (flags == nullptr || flags[pel] != 0u))')
     self.w(f'float* const col = {self._elem_ptr(out, "pel")} + (size_t)elj * {M}u;')
     if M % 4 == 0 and not s.accumulate:
       self.open('if ((reinterpret_cast<uintptr_t>(col) & 15u) == 0u)')
@@ -1079,6 +1155,8 @@ class _TC:
       self.w(f'for (int i = 0; i < {M}; ++i) col[i] = acc[i];')
     self.close()
     self.close()
+    if staged:
+      self.w('if (lane == 0) tfb_tc::bulk_wait();  // the last bulk stores have landed')
     self.close()
 
   # ------------------------------------------------------------------ producer

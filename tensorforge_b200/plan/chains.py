@@ -243,7 +243,10 @@ def _colprog_plan(chain, shape: LeftChain, fp_size, variant, threads):
   if a_total > COLPROG_MAX_FMAS and variant.get('strategy') != 'colprog':
     return None
   cols = int(variant.get('cols', 1))
-  te = tile_elements(shape, threads, cols)
+  rsplit = int(variant.get('rsplit', 1))
+  if rsplit > 1 and (shape.epilogue or threads % rsplit or shape.N > threads // rsplit):
+    rsplit = 1   # the elementwise epilogue needs whole columns in one thread
+  te = tile_elements(shape, threads // rsplit, cols)
   kmax = max(t.K for t in shape.terms)
   upitch = variant.get('upitch', 'odd' if a_source == 'mixed' else 'vec')
   pitch = (kmax | 1) if upitch == 'odd' else (kmax + vec - 1) // vec * vec + vec
@@ -269,7 +272,7 @@ def _colprog_plan(chain, shape: LeftChain, fp_size, variant, threads):
     return None
   # __launch_bounds__(128, 2) measured 4-5 % faster on the order-6 chain at every chunk size
   # (2.60e8 -> 2.70e8 el/s at chunk 16); 256-thread CTAs gain nothing from it
-  default_mb = 2 if threads == 128 else 0
+  default_mb = 2 if threads == 128 and rsplit == 1 else 0
   params = {'threads': threads, 'chunk': chunk, 'min_blocks': variant.get('min_blocks', default_mb),
             'a_source': a_source, 'prefetch': prefetch}
   if a_source == 'mixed':
@@ -278,6 +281,8 @@ def _colprog_plan(chain, shape: LeftChain, fp_size, variant, threads):
     params['upitch'] = upitch
   if cols != 1:
     params['cols'] = cols
+  if rsplit != 1:
+    params['rsplit'] = rsplit
   return Plan('colprog', params,
               smem, threads, note=f'M={shape.M} N={shape.N} terms={len(shape.terms)} tile={te}')
 

@@ -28,14 +28,60 @@ def small_specs(n, seed, hi=48, max_bytes=16 << 20):
   return random_chains(n, seed=seed, hi=hi, max_bytes=max_bytes)
 
 
+_SOURCE_HASH = []
+
+
+def _package_hash():
+  """Hash of the package's Python sources: a cached chain record is valid for one version."""
+  import hashlib
+  import os
+  if not _SOURCE_HASH:
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    h = hashlib.sha1()
+    for d, _, files in sorted(os.walk(root)):
+      if '_kcache' in d or '__pycache__' in d:
+        continue
+      for f in sorted(files):
+        if f.endswith('.py'):
+          with open(os.path.join(d, f), 'rb') as fh:
+            h.update(f.encode() + fh.read())
+    _SOURCE_HASH.append(h.hexdigest()[:16])
+  return _SOURCE_HASH[0]
+
+
+def _build_cached(spec, flags):
+  """build_chain with its record cached beside the library (generating ~20 variants in
+  Python costs seconds per chain; the record is keyed by the chain and the package sources)."""
+  import hashlib
+  import os
+  import pickle
+  from .autotune import build_chain
+  from .variants import space_signature
+  from ..runtime.build import CACHE
+  key = hashlib.sha1(f'{spec.key()}|{spec.seed}|{space_signature()}|{_package_hash()}|{flags}'.encode()).hexdigest()[:20]
+  path = os.path.join(CACHE, f'chain_{key}.pkl')
+  if os.path.exists(path):
+    with open(path, 'rb') as f:
+      cb = pickle.load(f)
+    if cb.so_path and os.path.exists(os.path.join(CACHE, os.path.basename(cb.so_path))):
+      cb.so_path = os.path.join(CACHE, os.path.basename(cb.so_path))
+      return cb
+  cb = build_chain(spec, extra_flags=flags)
+  os.makedirs(CACHE, exist_ok=True)
+  tmp = f'{path}.{os.getpid()}.tmp'
+  with open(tmp, 'wb') as f:
+    pickle.dump(cb, f)
+  os.replace(tmp, path)
+  return cb
+
+
 def build_all(specs, jobs=8):
   """Variant libraries of every chain (host work; nvcc runs in parallel; built without
   line information: they are timed, never profiled)."""
   from concurrent.futures import ThreadPoolExecutor
-  from .autotune import build_chain
   from ..runtime.build import NO_LINEINFO
   with ThreadPoolExecutor(max_workers=jobs) as pool:
-    return list(pool.map(lambda s: build_chain(s, extra_flags=(NO_LINEINFO,)), specs))
+    return list(pool.map(lambda s: _build_cached(s, (NO_LINEINFO,)), specs))
 
 
 def measure_all(builds, time_limit=None):

@@ -98,6 +98,8 @@ COLPROG_VARIANTS = [
   {'strategy': 'colprog', 'a_source': 'smem', 'cols': 2},
   {'strategy': 'colprog', 'a_source': 'const', 'prefetch': 0, 'threads': 256},
   {'strategy': 'colprog', 'a_source': 'mixed', 'const_terms': 1, 'upitch': 'odd', 'min_blocks': 3},
+  {'strategy': 'colprog', 'a_source': 'smem', 'threads': 256, 'rsplit': 2, 'min_blocks': 2},
+  {'strategy': 'colprog', 'a_source': 'smem', 'threads': 256, 'rsplit': 2, 'cols': 2},
 ]
 
 
