@@ -570,6 +570,17 @@ def impl_ours(args, rank, world, dist):
   opts_of = {'plain': {}, 'tf32x3': {'precision': 'tf32x3'},
              'tf32x3_ahead': {'precision': 'tf32x3', 'variant': {'form': 'u', 'ahead': 1}},
              'tf32x3_pipe2': {'precision': 'tf32x3', 'variant': {'form': 'u', 'pipe': 2}},
+             'tf32x3_s2': {'precision': 'tf32x3', 'variant': {'form': 'u', 'slots': 2}},
+             'tf32x3_nl': {'precision': 'tf32x3', 'variant': {'form': 'u', 'loader': 0}},
+             'tf32x3_u2': {'precision': 'tf32x3', 'variant': {'form': 'u', 'urows': 2}},
+             'tf32x3_q': {'precision': 'tf32x3', 'variant': {'form': 'u', 'qreg': 1}},
+             'tf32x3_q_s2': {'precision': 'tf32x3', 'variant': {'form': 'u', 'qreg': 1, 'slots': 2}},
+             'tf32x3_loader': {'precision': 'tf32x3', 'variant': {'form': 'u', 'loader': 1}},
+             'tf32x3_u2f': {'precision': 'tf32x3', 'variant': {'form': 'u', 'urows': 2, 'fuse': 1}},
+             'tf32x3_qf': {'precision': 'tf32x3', 'variant': {'form': 'u', 'qreg': 1, 'fuse': 1}},
+             'tf32x3_u2l': {'precision': 'tf32x3', 'variant': {'form': 'u', 'urows': 2, 'loader': 2}},
+             'tf32x3_u2fl': {'precision': 'tf32x3', 'variant': {'form': 'u', 'urows': 2, 'fuse': 1, 'loader': 2}},
+
              'plain_rs2': {'variant': {'strategy': 'colprog', 'threads': 256, 'rsplit': 2, 'min_blocks': 2}},
              'tf32x3_form_b': {'precision': 'tf32x3', 'variant': {'form': 'b'}},
              'tf32x3_form_b2': {'precision': 'tf32x3', 'variant': {'form': 'b', 'bbuf': 2}},

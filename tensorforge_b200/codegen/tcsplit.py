@@ -146,24 +146,41 @@ def smem_plan_v2(shape, precision):
               pitch=pitch, ubuf_bytes=ubuf, off_bar=off_bar, total=total, te=te, tc=tc)
 
 
-def smem_plan_v3(shape, precision):
-  """Shared memory of the warp-specialised pipeline: the one-pass layout with the B operand
-  stored for the real output rows only (rows M..N_mma-1 of the MMA's B tile then read the
-  next block, and land in accumulator columns the epilogue never reads) and, when it fits,
-  an output staging buffer for the epilogue warps' bulk stores."""
+def smem_plan_v3(shape, precision, qreg=False, fuse=False):
+  """Shared memory of the warp-specialised pipeline: the one-pass layout, an output staging
+  buffer for the epilogue warps' bulk stores (32 rows per warp, or 16 rows at a time when
+  only that fits) and the B operand. Without `fuse` B is stored for the real output rows
+  only (rows M..N_mma-1 of the MMA's B tile then read the next block and land in
+  accumulator columns the epilogue never reads); with `fuse` each term's hi and lo blocks
+  are whole N_mma-row tiles, back to back, read by one MMA of width 2 N_mma."""
   sm = smem_plan_v2(shape, precision)
+  if qreg:
+    # the stage holds the R blocks only (B is read into registers)
+    off = 0
+    stage_off = {}
+    for op in sm['r_ops']:
+      stage_off[op.name] = off
+      off += sm['te'] * _pad(op.storage_size() if op.sparse else op.element_volume(), 4)
+    stage = _pad(off * 4, 128)
+    shrink = sm['stage'] - stage
+    sm = dict(sm, stage=stage, stage_off=stage_off, off_u=sm['off_u'] - shrink, off_bar=sm['off_bar'] - shrink,
+              total=sm['total'] - shrink)
   lay = layout(shape, precision)
-  rows_b = _pad(shape.M, 8)
+  rows_b = lay['n_mma'] if fuse else _pad(shape.M, 8)
   b_bytes = sum(2 * rows_b * kp * lay['es'] for kp in lay['kpad'])
   shift = sm['off_stage'] - _pad(b_bytes, 128)
-  out = dict(sm, rows_b=rows_b, b_bytes=b_bytes)
+  out = dict(sm, rows_b=rows_b, b_bytes=b_bytes, ost_rows=0)
   for k in ('off_stage', 'off_u', 'off_bar', 'total'):
     out[k] = sm[k] - shift
-  ost = _pad(sm['tc'] * shape.M * 4, 128)
-  if shape.M % 4 == 0 and out['total'] + ost <= _plan.SMEM_LIMIT:
-    out['off_ost'] = out['off_bar']
-    out['off_bar'] += ost
-    out['total'] += ost
+  if shape.M % 4 == 0:
+    for rows in (32, 16):
+      ost = _pad(4 * rows * shape.M * 4, 128)
+      if out['total'] + ost <= _plan.SMEM_LIMIT:
+        out['off_ost'] = out['off_bar']
+        out['off_bar'] += ost
+        out['total'] += ost
+        out['ost_rows'] = rows
+        break
   return out
 
 
@@ -178,7 +195,8 @@ def pipe3_ok(shape, precision, chunk=16):
     return False
   if any(-(-kp // 16) > H_GROUPS for kp in lay['kpad']):
     return False
-  return 4 * max(lay['a_cols']) + 4 * lay['n_mma'] <= 512
+  return 4 * max(lay['a_cols']) + 4 * lay['n_mma'] <= 512 or (
+    2 * len(shape.terms) * max(lay['a_cols']) + 2 * lay['n_mma'] <= 512)
 
 
 def plan(chain, shape, precision, variant):
@@ -222,7 +240,16 @@ def plan(chain, shape, precision, variant):
   pipe = variant.get('pipe', default_pipe)
   if pipe == 3 and not pipe3_ok(shape, precision, variant.get('chunk', 16)):
     pipe = 2
-  sm = (smem_plan_v3 if pipe == 3 else smem_plan_v2)(shape, precision) if pipe in (2, 3) else None
+  fuse = 0
+  if pipe == 3:
+    # defaults of the warp-specialised pipeline (measured on the order-6 chain, 500,000
+    # elements: 6.37e8 el/s against 6.28e8 without the fused MMA and the bulk loader warp,
+    # 5.67e8 with one U row per producer): two U rows per producer, the hi*hi and hi*lo
+    # products as one MMA of twice the width when the whole B tiles fit
+    qreg = bool(int(variant.get('qreg', 0)))
+    fuse = int(variant.get('fuse', 1 if smem_plan_v3(shape, precision, qreg, True)['total'] <= _plan.SMEM_LIMIT else 0))
+  sm = ((lambda sh, pr: smem_plan_v3(sh, pr, bool(int(variant.get('qreg', 0))), bool(fuse)))
+        if pipe == 3 else smem_plan_v2)(shape, precision) if pipe in (2, 3) else None
   if sm is None or sm['total'] > _plan.SMEM_LIMIT:
     pipe = 1
     sm = smem_plan(shape, precision)
@@ -233,7 +260,35 @@ def plan(chain, shape, precision, variant):
   params = {'precision': precision, 'chunk': chunk, 'pipe': pipe}
   if int(variant.get('ahead', 0)) and pipe == 2:
     params['ahead'] = 1
-  if int(variant.get('urows', 1)) == 2 and pipe in (2, 3) and all(t.K % 2 == 0 for t in shape.terms):
+  if pipe == 3:
+    # A slots: one per term when the tensor memory also holds one accumulator pair (no
+    # lane phase then waits for a slot), else two slots and two accumulator pairs
+    lay3 = layout(shape, precision)
+    scols = 2 * max(lay3['a_cols'])
+    dcols = 2 * lay3['n_mma']
+    nt = len(shape.terms)
+    fit_one = nt * scols + dcols <= 512
+    ns = int(variant.get('slots', nt if fit_one else 2))
+    if ns not in (2, nt) or ns * scols + (1 if ns == nt else 2) * dcols > 512:
+      ns = 2
+    params['slots'] = ns
+    # loader warp: 2 (default) issues only the bulk copy of the B blocks, the producers keep
+    # the small R copies; 1 fetches all inputs (measured slower: 4.8e8 el/s, the stage is
+    # single-buffered and one warp issues the R copies slowly); 0 none
+    params['loader'] = int(variant.get('loader', 2))
+    # option: the per-element B operand goes straight from global memory into registers one
+    # tile ahead (two rows per producer), so the stage only holds the R blocks
+    b_ops = {id(t.B) for t in shape.terms}
+    if (int(variant.get('qreg', 0)) and not params['loader'] and len(b_ops) == 1
+        and all(t.K % 2 == 0 for t in shape.terms)
+        and lay3['te'] * shape.terms[0].K // 2 <= 128 * H_GROUPS):
+      params['qreg'] = 1
+      params['urows'] = 2
+  if pipe == 3 and fuse:
+    # hi*hi and hi*lo as one MMA of twice the width (B's hi and lo tiles back to back, the
+    # main and correction accumulators side by side)
+    params['fuse'] = 1
+  if int(variant.get('urows', 2 if pipe == 3 else 1)) == 2 and pipe in (2, 3) and all(t.K % 2 == 0 for t in shape.terms):
     params['urows'] = 2
   if int(variant.get('wait_probe', 0)) > 0:
     # failure-detection check: the kernel first waits, with this many polls, on an mbarrier
@@ -383,8 +438,10 @@ class _TC:
     self.prec = plan_.params['precision']
     self.lay = layout(shape, self.prec)
     self.pipe = plan_.params.get('pipe', 1)
-    self.sm = ({3: smem_plan_v3, 2: smem_plan_v2}[self.pipe](shape, self.prec) if self.pipe in (2, 3)
-               else smem_plan(shape, self.prec))
+    self.qreg = self.pipe == 3 and int(plan_.params.get('qreg', 0)) == 1
+    self.fuse = self.pipe == 3 and int(plan_.params.get('fuse', 0)) == 1
+    self.sm = (smem_plan_v3(shape, self.prec, self.qreg, self.fuse) if self.pipe == 3 else
+               smem_plan_v2(shape, self.prec) if self.pipe == 2 else smem_plan(shape, self.prec))
     self.LC = plan_.params['chunk']
     self.ahead = bool(plan_.params.get('ahead', 0))
     self.H = H_GROUPS
@@ -496,20 +553,32 @@ class _TC:
     d_main, d_corr = col, col + n_mma
     lim = self.WAIT_LIMIT
     p3 = self.pipe == 3
-    nthreads = 32 * (4 * H + 1 + (4 if p3 else 0))
+    # loader warp: 1 fetches all inputs of the next tile, 2 only the bulk copy of the B
+    # blocks (the producers keep issuing the small R copies)
+    self.loader_mode = int(self.plan.params.get('loader', 0)) if p3 else 0
+    self.loader = self.loader_mode in (1, 2)
+    nthreads = 32 * (4 * H + 1 + (4 if p3 else 0) + (1 if self.loader else 0))
     BAR_FULL, BAR_FREE, BAR_DFULL, BAR_DFREE = 0, nterms, 2 * nterms, 2 * nterms + 1
     if p3:
-      # two A slots used in turn by the terms of consecutive tiles, two accumulator pairs
+      # NS A slots used in turn by the terms (chunk c = it * terms + t takes slot c % NS),
+      # ND accumulator pairs (tile it takes pair it % ND)
+      self.NS = int(self.plan.params.get('slots', 2))
+      self.ND = 1 if self.NS == nterms else 2
+      self.dcols = 2 * n_mma
       self.scols = 2 * max(lay['a_cols'])
-      self.d_base = 2 * self.scols
-      BAR_FULL, BAR_FREE, BAR_DFULL, BAR_DFREE = 0, 2, 4, 6
+      self.d_base = self.NS * self.scols
+      assert self.d_base + self.ND * self.dcols <= 512
+      BAR_FULL, BAR_FREE = 0, self.NS
+      BAR_DFULL, BAR_DFREE = 2 * self.NS, 2 * self.NS + self.ND
+      self.BAR = dict(full=BAR_FULL, free=BAR_FREE, dfull=BAR_DFULL, dfree=BAR_DFREE,
+                      stage=2 * self.NS + 2 * self.ND, sfree=2 * self.NS + 2 * self.ND + 1)
 
     self.w(f'__global__ void __launch_bounds__({nthreads}, 1) {kname}({", ".join(self.params(globals_))}) {{')
     self.ind += 1
     self.w('extern __shared__ __align__(1024) unsigned char tfb_smem_raw[];')
     self.w(f'uint64_t* const bars = reinterpret_cast<uint64_t*>(tfb_smem_raw + {sm["off_bar"]});')
-    nbars = 9 if p3 else 2 * nterms + (3 if self.pipe == 2 else 2)
-    BAR_STAGE = 8 if p3 else 2 * nterms + 2
+    nbars = (2 * self.NS + 2 * self.ND + 2) if p3 else 2 * nterms + (3 if self.pipe == 2 else 2)
+    BAR_STAGE = self.BAR['stage'] if p3 else 2 * nterms + 2
     self.w(f'unsigned* const tmem_slot = reinterpret_cast<unsigned*>(bars + {nbars});')
     probe = int(self.plan.params.get('wait_probe', 0))
     if probe:
@@ -549,11 +618,14 @@ class _TC:
       self.close()
     self.open('if (threadIdx.x == 0)')
     if p3:
-      for i in range(2):
+      for i in range(self.NS):
         self.w(f'tfb_tc::mbar_init(&bars[{BAR_FULL + i}], {NP}u);')
         self.w(f'tfb_tc::mbar_init(&bars[{BAR_FREE + i}], 1u);')
+      for i in range(self.ND):
         self.w(f'tfb_tc::mbar_init(&bars[{BAR_DFULL + i}], 1u);')
         self.w(f'tfb_tc::mbar_init(&bars[{BAR_DFREE + i}], 128u);')
+      if self.loader:
+        self.w(f'tfb_tc::mbar_init(&bars[{self.BAR["sfree"]}], 1u);')
     else:
       for ti in range(nterms):
         self.w(f'tfb_tc::mbar_init(&bars[{BAR_FULL + ti}], {NP}u);')
@@ -561,8 +633,8 @@ class _TC:
       self.w(f'tfb_tc::mbar_init(&bars[{BAR_DFULL}], 1u);')
       self.w(f'tfb_tc::mbar_init(&bars[{BAR_DFREE}], {NP}u);')
     if self.pipe in (2, 3):
-      # one arrival per producer (cp.async completion) + the bulk-copy issuer's expect_tx
-      self.w(f'tfb_tc::mbar_init(&bars[{BAR_STAGE}], {NP + 1}u);')
+      # one arrival per copying thread (cp.async completion) + the bulk-copy issuer's expect_tx
+      self.w(f'tfb_tc::mbar_init(&bars[{BAR_STAGE}], {(32 if self.loader_mode == 1 else NP) + 1}u);')
     if probe:
       self.w('tfb_tc::mbar_init(probe_bar, 1u);')
     self.w('asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");')
@@ -619,6 +691,8 @@ class _TC:
     if p3:
       self._producers_v3(s, te, tcols, NP, stage_off, lim, BAR_STAGE)
       self._epilogue_warps_v3(s, te, tcols, lim, n_mma)
+      if self.loader:
+        self._loader_v3(stage_off, lim, BAR_STAGE)
     elif self.pipe == 2:
       self._producers_v2(s, te, tcols, NP, stage_off, slot_base, lim, BAR_DFULL, BAR_STAGE, d_main, d_corr)
     else:
@@ -773,7 +847,7 @@ class _TC:
       self.close()
     self.close()
 
-  def _loads_v2(self, tile_expr, part, stage_off, BAR_STAGE, NP):
+  def _loads_v2(self, tile_expr, part, stage_off, BAR_STAGE, NP, sync=True):
     """Inputs of tile `tile_expr` into the stage. part 1: the R blocks (cp.async by every
     producer; their region never overlaps the staged output). part 2: the B blocks, one
     bulk copy each when every block is contiguous and 16-byte aligned (issued by producer 0
@@ -807,7 +881,8 @@ class _TC:
     self.close()
     self.close()
     self.open('else')
-    self.w(f'tfb_tc::named_sync(1, {NP});  // the previous tile\'s staged output has been read')
+    if sync:
+      self.w(f'tfb_tc::named_sync(1, {NP});  // the previous tile\'s staged output has been read')
     for op in b_ops:
       self._cp_async_copy(op, op.element_volume(), stage_off[op.name], tile_expr, 'stage', NP)
     self.w(f'if (ptid == 0) tfb_tc::mbar_arrive(&bars[{BAR_STAGE}]);')
@@ -940,23 +1015,23 @@ class _TC:
     self.close()
 
   # ------------------------------------------------------------------ warp-specialised pipeline
-  # Barriers: FULL[0..1] (A slot written, NP arrivals), FREE[0..1] (A slot read by the MMAs,
-  # one commit), DFULL[0..1] (accumulator pair complete, one commit), DFREE[0..1]
-  # (accumulator pair read, 128 epilogue arrivals), STAGE (inputs landed). Term t of the
-  # CTA's it-th tile is chunk c = it * terms + t and uses A slot c % 2; tile it uses
-  # accumulator pair it % 2.
+  # Barriers: FULL[NS] (A slot written, NP arrivals), FREE[NS] (A slot read by the MMAs, one
+  # commit), DFULL[ND] (accumulator pair complete, one commit), DFREE[ND] (accumulator pair
+  # read, 128 epilogue arrivals), STAGE (inputs landed), SFREE (stage consumed by the U pass,
+  # for the loader warp). Term t of the CTA's it-th tile is chunk c = it * terms + t and uses
+  # A slot c % NS (its (c / NS)-th use); tile it uses accumulator pair it % ND.
   def _mma_v3(self, s, lay, b_off, ke, es, idesc, lim, n_mma):
     b = self.base
-    nterms = len(s.terms)
+    NS, ND, B = self.NS, self.ND, self.BAR
     mma = 'mma_tf32' if self.prec == 'tf32x3' else 'mma_f16'
     half = self.scols // 2
     self.open(f'if (warp == {4 * self.H})')
     self.open('if (lane == 0)')
     self.w('unsigned it = 0, chunk = 0;')
     self.open('for (size_t tile = blockIdx.x; tile < numTiles && ok; tile += gridDim.x, ++it)')
-    self.w('const unsigned db = it & 1u;')
-    self.w(f'const unsigned d_main = tmem + {self.d_base}u + db * {2 * n_mma}u, d_corr = d_main + {n_mma}u;')
-    self.w(f'if (it >= 2u && !tfb_tc::mbar_wait(&bars[6u + db], ((it - 2u) >> 1) & 1u, {lim}ull)) '
+    self.w(f'const unsigned db = it % {ND}u;')
+    self.w(f'const unsigned d_main = tmem + {self.d_base}u + db * {self.dcols}u, d_corr = d_main + {n_mma}u;')
+    self.w(f'if (it >= {ND}u && !tfb_tc::mbar_wait(&bars[{B["dfree"]}u + db], ((it - {ND}u) / {ND}u) & 1u, {lim}ull)) '
            f'{{ ok = false; atomicMax(&tfb_err_{b}, 13u); break; }}')
     self.w('tfb_tc::fence_after();')
     for ti, t in enumerate(s.terms):
@@ -966,8 +1041,9 @@ class _TC:
       sbo = (kp // ke) * 128
       cps = lay['ks'] * es // 4
       self.w('{')
-      self.w('const unsigned sl = chunk & 1u;')
-      self.w(f'if (!tfb_tc::mbar_wait(&bars[sl], (chunk >> 1) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, {10 + ti}u); break; }}')
+      self.w(f'const unsigned sl = chunk % {NS}u;')
+      self.w(f'if (!tfb_tc::mbar_wait(&bars[{B["full"]}u + sl], (chunk / {NS}u) & 1u, {lim}ull)) '
+             f'{{ ok = false; atomicMax(&tfb_err_{b}, {10 + ti}u); break; }}')
       self.w('tfb_tc::fence_after();')
       self.open(f'for (int ks = 0; ks < {ksteps}; ++ks)')
       self.w(f'const unsigned a_hi = tmem + sl * {self.scols}u + ks * {cps}u;')
@@ -975,27 +1051,34 @@ class _TC:
       self.w(f'const uint64_t bh = tfb_tc::smem_desc(tfb_tc::smem_u32(tfb_smem_raw + {hi_off}) + ks * 256u, 128u, {sbo}u);')
       self.w(f'const uint64_t bl = tfb_tc::smem_desc(tfb_tc::smem_u32(tfb_smem_raw + {lo_off}) + ks * 256u, 128u, {sbo}u);')
       first = '(ks > 0) ? 1u : 0u' if ti == 0 else '1u'
-      self.w(f'tfb_tc::{mma}(d_main, a_hi, bh, {idesc}u, {first});')
-      self.w(f'tfb_tc::{mma}(d_corr, a_hi, bl, {idesc}u, {first});')
+      if self.fuse:
+        # B rows [0, N) hi and [N, 2N) lo: one MMA writes main and correction side by side
+        assert b_off[ti][1] - b_off[ti][0] == n_mma * kp * es
+        idesc2 = (idesc & ~(0x3F << 17)) | (((2 * n_mma) >> 3) << 17)
+        self.w(f'tfb_tc::{mma}(d_main, a_hi, bh, {idesc2}u, {first});')
+      else:
+        self.w(f'tfb_tc::{mma}(d_main, a_hi, bh, {idesc}u, {first});')
+        self.w(f'tfb_tc::{mma}(d_corr, a_hi, bl, {idesc}u, {first});')
       self.w(f'tfb_tc::{mma}(d_corr, a_lo, bh, {idesc}u, 1u);')
       self.close()
-      self.w('tfb_tc::mma_commit(&bars[2u + sl]);')
+      self.w(f'tfb_tc::mma_commit(&bars[{B["free"]}u + sl]);')
       self.w('++chunk;')
       self.w('}')
-    self.w('tfb_tc::mma_commit(&bars[4u + db]);')
+    self.w(f'tfb_tc::mma_commit(&bars[{B["dfull"]}u + db]);')
     self.close()
     self.close()
     self.close()
 
   def _lane_v3(self, ti, t, lim, src, nterms):
-    """Lane phase of term ti into A slot (chunk % 2): wait until the MMAs of the chunk two
+    """Lane phase of term ti into A slot (chunk % NS): wait until the MMAs of the chunk NS
     before have read the slot, split the lane's column of U_t and store hi / lo."""
     b = self.base
+    NS, B = self.NS, self.BAR
     kp = self.lay['kpad'][ti]
     half = self.scols // 2
     self.open('')
-    self.w(f'const unsigned chunk = it * {nterms}u + {ti}u, sl = chunk & 1u;')
-    self.w(f'if (chunk >= 2u && !tfb_tc::mbar_wait(&bars[2u + sl], ((chunk - 2u) >> 1) & 1u, {lim}ull)) '
+    self.w(f'const unsigned chunk = it * {nterms}u + {ti}u, sl = chunk % {NS}u;')
+    self.w(f'if (chunk >= {NS}u && !tfb_tc::mbar_wait(&bars[{B["free"]}u + sl], ((chunk - {NS}u) / {NS}u) & 1u, {lim}ull)) '
            f'{{ ok = false; atomicMax(&tfb_err_{b}, {30 + ti}u); }}')
     self.w('tfb_tc::fence_after();')
     self.w(f'const unsigned slot = lane_addr + sl * {self.scols}u;')
@@ -1022,13 +1105,14 @@ class _TC:
     self.close()
     self.w('tfb_tc::st_wait();')
     self.w('tfb_tc::fence_before();')
-    self.w('tfb_tc::mbar_arrive(&bars[sl]);')
+    self.w(f'tfb_tc::mbar_arrive(&bars[{B["full"]}u + sl]);')
     self.close()
 
   def _producers_v3(self, s, te, tcols, NP, stage_off, lim, BAR_STAGE):
     """Producer warps of the warp-specialised pipeline. Per tile: [barrier: abort OR] wait
-    for the stage, U pass of all terms, [barrier], loads of the next tile into the stage,
-    lane phases of the terms into the A slots. The epilogue runs on its own warps."""
+    for the stage, U pass of all terms, [barrier], release the stage (to the loader warp, or
+    issue the next tile's loads), lane phases of the terms into the A slots. The epilogue
+    runs on its own warps."""
     b, H = self.base, self.H
     pitch = self.sm['pitch']
     nterms = len(s.terms)
@@ -1040,36 +1124,188 @@ class _TC:
     self.w(f'const bool lane_col = row < {tcols}u;')
     self.w(f'const unsigned le = row / {s.N}u;')
     self.w('unsigned it = 0;')
-    self.w('bool pending = false;')
-    self.open('if (blockIdx.x < numTiles)')
-    self._loads_v2('(size_t)blockIdx.x', 1, stage_off, BAR_STAGE, NP)
-    self._loads_v2('(size_t)blockIdx.x', 2, stage_off, BAR_STAGE, NP)
-    self.w('pending = true;')
-    self.close()
+    if self.qreg:
+      self._q_decl()
+    rcopies = self.loader_mode != 1   # the producers copy the R blocks
+    if rcopies:
+      self.w('bool pending = false;')
+      self.open('if (blockIdx.x < numTiles)')
+      self._loads_v2('(size_t)blockIdx.x', 1, stage_off, BAR_STAGE, NP)
+      if self.loader_mode == 2:
+        self.w(f'tfb_tc::cp_async_mbar_arrive(&bars[{BAR_STAGE}]);')
+      elif self.qreg:
+        self._q_load('(size_t)blockIdx.x')
+        self.w(f'if (ptid == 0) tfb_tc::mbar_arrive(&bars[{BAR_STAGE}]);')
+        self.w(f'tfb_tc::cp_async_mbar_arrive(&bars[{BAR_STAGE}]);')
+      else:
+        self._loads_v2('(size_t)blockIdx.x', 2, stage_off, BAR_STAGE, NP)
+      self.w('pending = true;')
+      self.close()
     self.open('for (size_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++it)')
     self.w('// every producer takes the same branches around named barriers: a timeout anywhere')
     self.w('// stops all producers at the next tile boundary (a barrier-wide OR), never mid-tile')
     self.w(f'if (tfb_tc::any_sync(1, {NP}, !ok)) break;')
-    self.w('const size_t ntile = tile + gridDim.x;')
-    self.w('const bool has_next = ntile < numTiles;')
     self.w(f'if (!tfb_tc::mbar_wait(&bars[{BAR_STAGE}], it & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 40u); }}')
-    self.w('pending = false;')
-    self._u_phase_v2(stage_off, NP)
+    if rcopies:
+      self.w('const size_t ntile = tile + gridDim.x;')
+      self.w('const bool has_next = ntile < numTiles;')
+      self.w('pending = false;')
+    if self.qreg:
+      self._u_phase_qreg(stage_off, NP)
+      self.open('if (has_next)')
+      self._q_load('ntile')   # in flight during this tile's lane phases
+      self.close()
+    else:
+      self._u_phase_v2(stage_off, NP)
     self.w(f'tfb_tc::named_sync(1, {NP});')
-    self.open('if (has_next)')
-    self._loads_v2('ntile', 1, stage_off, BAR_STAGE, NP)
-    self._loads_v2('ntile', 2, stage_off, BAR_STAGE, NP)
-    self.w('pending = true;')
-    self.close()
+    if self.loader:
+      self.w(f'if (ptid == 0) tfb_tc::mbar_arrive(&bars[{self.BAR["sfree"]}]);  // the stage is free for the loader')
+    if rcopies:
+      self.open('if (has_next)')
+      self._loads_v2('ntile', 1, stage_off, BAR_STAGE, NP)
+      if self.loader_mode == 2:
+        self.w(f'tfb_tc::cp_async_mbar_arrive(&bars[{BAR_STAGE}]);')
+      elif self.qreg:
+        self.w(f'if (ptid == 0) tfb_tc::mbar_arrive(&bars[{BAR_STAGE}]);')
+        self.w(f'tfb_tc::cp_async_mbar_arrive(&bars[{BAR_STAGE}]);')
+      else:
+        self._loads_v2('ntile', 2, stage_off, BAR_STAGE, NP)
+      self.w('pending = true;')
+      self.close()
     self.w(f'const size_t el = tile * {te}u + le;')
     self.w('const bool active = lane_col && el < numElements && (flags == nullptr || flags[el] != 0u);')
     for ti, t in enumerate(s.terms):
       self._lane_v3(ti, t, lim, f'(ubuf{ti} + row * {pitch}u)', nterms)
     self.close()
-    self.w('// a stage load still in flight after an abort must land before the CTA exits')
-    self.w(f'if (pending && !tfb_tc::mbar_wait(&bars[{BAR_STAGE}], it & 1u, {lim}ull)) atomicMax(&tfb_err_{b}, 41u);')
+    if rcopies:
+      self.w('// a stage load still in flight after an abort must land before the CTA exits')
+      self.w(f'if (pending && !tfb_tc::mbar_wait(&bars[{BAR_STAGE}], it & 1u, {lim}ull)) atomicMax(&tfb_err_{b}, 41u);')
+      self.w('tfb_tc::cp_async_wait_all();')
+      self.w('if (ptid == 0) tfb_tc::bulk_wait();')
+    self.close()
+
+  def _q_decl(self):
+    """Registers holding this producer's two rows of the (single) B operand for one tile."""
+    t0 = self.s.terms[0]
+    self.w(f'float2 qv[{t0.P}];')
+    self.w('#pragma unroll')
+    self.w(f'for (int m = 0; m < {t0.P}; ++m) qv[m] = make_float2(0.0f, 0.0f);')
+
+  def _q_load(self, tile_expr):
+    """Rows l, l + 1 of B for producer item ptid of tile `tile_expr`, straight from global
+    memory (64-bit loads when 8-byte aligned), zeros past the last element."""
+    s = self.s
+    t0 = s.terms[0]
+    B, K, P = t0.B, t0.K, t0.P
+    te = self.sm['te']
+    self.open('')
+    self.w(f'const unsigned ei = ptid / {K // 2}u, l = 2u * (ptid - ei * {K // 2}u);')
+    self.w(f'const size_t e = ({tile_expr}) * {te}u + ei;')
+    self.open(f'if (ptid < {te * K // 2}u && e < numElements)')
+    self.w(f'const float* const src = {self._elem_ptr(B, "e")} + l;')
+    self.open('if ((reinterpret_cast<uintptr_t>(src) & 7u) == 0u)')
+    self.w('#pragma unroll')
+    self.w(f'for (int m = 0; m < {P}; ++m) qv[m] = __ldg(reinterpret_cast<const float2*>(src + m * {K}));')
+    self.close()
+    self.open('else')
+    self.w('#pragma unroll')
+    self.w(f'for (int m = 0; m < {P}; ++m) qv[m] = make_float2(__ldg(src + m * {K}), __ldg(src + m * {K} + 1));')
+    self.close()
+    self.close()
+    self.open('else')
+    self.w('#pragma unroll')
+    self.w(f'for (int m = 0; m < {P}; ++m) qv[m] = make_float2(0.0f, 0.0f);')
+    self.close()
+    self.close()
+
+  def _u_phase_qreg(self, stage_off, NP):
+    """U pass from the B rows in registers: producer ptid < te * K / 2 computes rows l, l + 1
+    of every U_t (R_t from the stage, pattern unrolled) with 64-bit stores."""
+    s, sm = self.s, self.sm
+    te, pitch, N = sm['te'], sm['pitch'], s.N
+    comp = ['x', 'y', 'z', 'w']
+    K = s.terms[0].K
+    self.open(f'if (ptid < {te * K // 2}u)')
+    self.w(f'const unsigned ei = ptid / {K // 2}u, l = 2u * (ptid - ei * {K // 2}u);')
+    for ti, t in enumerate(s.terms):
+      dst = f'ubuf{ti}[(ei * {N}u + {{j}}u) * {pitch}u + l]'
+      nr = t.R.storage_size()
+      self.open('')
+      self.w(f'const float4* const rq = reinterpret_cast<const float4*>(stage + {stage_off[t.R.name]} + ei * {_pad(nr, 4)}u);')
+      for v in range((nr + 3) // 4):
+        self.w(f'const float4 r{v} = rq[{v}];')
+      look = t.R.sparse_lookup() if t.R.sparse else None
+      for j in range(N):
+        ex, ey = '0.0f', '0.0f'
+        for m in range(t.P):
+          pos = look.get((m, j)) if look is not None else j * t.P + m
+          if pos is not None:
+            r = f'r{pos // 4}.{comp[pos % 4]}'
+            ex = f'fmaf(qv[{m}].x, {r}, {ex})'
+            ey = f'fmaf(qv[{m}].y, {r}, {ey})'
+        self.w(f'*reinterpret_cast<float2*>(&{dst.format(j=j)}) = make_float2({ex}, {ey});')
+      self.close()
+    self.close()
+
+  def _bulk_b_only(self, tile_expr, stage_off, BAR_STAGE):
+    """Loader mode 2: the B blocks of a tile, one bulk copy by lane 0 with its expect_tx
+    arrival; when a block is misaligned the 32 lanes copy it with cp.async, wait for their
+    copies and lane 0 arrives (one arrival either way)."""
+    sm = self.sm
+    te = sm['te']
+    b_ops = sm['b_ops']
+    eligible = all(_bulk_eligible(op, op.element_volume()) for op in b_ops)
+    self.open('')
+    self.w(f'const size_t be0 = ({tile_expr}) * {te}u;')
+    self.w(f'const unsigned bnv = (unsigned)((numElements - be0) < {te}u ? (numElements - be0) : {te}u);')
+    if eligible:
+      conds = ' && '.join(f'((reinterpret_cast<uintptr_t>({op.name} + be0 * {op.element_volume()}u + '
+                          f'{op.name}_extraOffset) & 15u) == 0u)' for op in b_ops)
+      self.w(f'const bool bulk_in = {conds};')
+    else:
+      self.w('const bool bulk_in = false;')
+    per_elem = sum(op.element_volume() * 4 for op in b_ops)
+    self.open('if (bulk_in)')
+    self.open('if (lane == 0)')
+    self.w(f'tfb_tc::mbar_arrive_expect_tx(&bars[{BAR_STAGE}], bnv * {per_elem}u);')
+    for op in b_ops:
+      self.w(f'tfb_tc::bulk_load(stage + {stage_off[op.name]}, {op.name} + be0 * {op.element_volume()}u + '
+             f'{op.name}_extraOffset, bnv * {op.element_volume() * 4}u, &bars[{BAR_STAGE}]);')
+    self.close()
+    self.close()
+    self.open('else')
+    for op in b_ops:
+      self._cp_async_copy(op, op.element_volume(), stage_off[op.name], tile_expr, 'stage', 32)
     self.w('tfb_tc::cp_async_wait_all();')
-    self.w('if (ptid == 0) tfb_tc::bulk_wait();')
+    self.w('__syncwarp();')
+    self.w(f'if (lane == 0) tfb_tc::mbar_arrive(&bars[{BAR_STAGE}]);')
+    self.close()
+    self.close()
+
+  def _loader_v3(self, stage_off, lim, BAR_STAGE):
+    """Loader warp: fetches each tile's inputs into the stage (bulk copy of the B blocks by
+    lane 0, cp.async of the R blocks by the 32 lanes) as soon as the producers have released
+    it, so the producers never issue copies themselves."""
+    b = self.base
+    self.open('else')
+    self.w('const unsigned ptid = lane;')
+    self.w('unsigned it = 0;')
+    self.w('bool pending = false;')
+    self.open('for (size_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++it)')
+    self.w(f'if (it > 0u && !tfb_tc::mbar_wait(&bars[{self.BAR["sfree"]}], (it - 1u) & 1u, {lim}ull)) '
+           f'{{ ok = false; atomicMax(&tfb_err_{b}, 42u); break; }}')
+    if self.loader_mode == 1:
+      self._loads_v2('tile', 1, stage_off, BAR_STAGE, 32)
+      self._loads_v2('tile', 2, stage_off, BAR_STAGE, 32, sync=False)
+    else:
+      self._bulk_b_only('tile', stage_off, BAR_STAGE)
+    self.w('pending = true;')
+    self.close()
+    self.w('// copies still in flight must land before the CTA exits: the last tile\'s, consumed')
+    self.w('// by the producers, or one nobody consumed after an abort')
+    self.w(f'if (pending && !tfb_tc::mbar_wait(&bars[{BAR_STAGE}], (it - 1u) & 1u, {lim}ull)) atomicMax(&tfb_err_{b}, 41u);')
+    self.w('tfb_tc::cp_async_wait_all();')
+    self.w('if (lane == 0) tfb_tc::bulk_wait();')
     self.close()
 
   def _epilogue_warps_v3(self, s, te, tcols, lim, n_mma):
@@ -1080,7 +1316,7 @@ class _TC:
     M = s.M
     out = s.out
     nld = (M + 7) // 8
-    self.open('else')
+    self.open(f'else if (warp < {4 * self.H + 5})' if self.loader else 'else')
     self.w('const unsigned equad = warp & 3u;')
     self.w('const unsigned erow = equad * 32u + lane;')
     self.w('const unsigned e_addr = tmem + ((equad * 32u) << 16);')
@@ -1088,10 +1324,11 @@ class _TC:
     self.w(f'const unsigned ele = erow / {s.N}u, elj = erow - ele * {s.N}u;')
     self.w('unsigned it = 0;')
     self.open('for (size_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++it)')
-    self.w('const unsigned db = it & 1u;')
-    self.w(f'if (!tfb_tc::mbar_wait(&bars[4u + db], (it >> 1) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 20u); break; }}')
+    self.w(f'const unsigned db = it % {self.ND}u;')
+    self.w(f'if (!tfb_tc::mbar_wait(&bars[{self.BAR["dfull"]}u + db], (it / {self.ND}u) & 1u, {lim}ull)) '
+           f'{{ ok = false; atomicMax(&tfb_err_{b}, 20u); break; }}')
     self.w('tfb_tc::fence_after();')
-    self.w(f'const unsigned dm = e_addr + {self.d_base}u + db * {2 * n_mma}u;')
+    self.w(f'const unsigned dm = e_addr + {self.d_base}u + db * {self.dcols}u;')
     self.w(f'float acc[{nld * 8}];')
     for k0 in range(0, nld, 2):
       ks = list(range(k0, min(nld, k0 + 2)))
@@ -1105,7 +1342,7 @@ class _TC:
       self.w(f'for (int i = 0; i < {8 * len(ks)}; ++i) acc[{8 * k0} + i] = __uint_as_float(dv[i]) + __uint_as_float(dc[i]);')
       self.close()
     self.w('tfb_tc::fence_before();')
-    self.w('tfb_tc::mbar_arrive(&bars[6u + db]);')
+    self.w(f'tfb_tc::mbar_arrive(&bars[{self.BAR["dfree"]}u + db]);')
     self.w(f'const size_t pel = tile * {te}u + ele;')
     staged = ('off_ost' in self.sm and out.addressing.name == 'STRIDED' and not s.accumulate
               and out.element_volume() == M * s.N and M % 4 == 0)
@@ -1116,22 +1353,26 @@ class _TC:
       self.w(f'float* const obase = {out.name} + tile * {te * vol}u + {out.name}_extraOffset;')
       self.open('if (flags == nullptr && (reinterpret_cast<uintptr_t>(obase) & 15u) == 0u)')
       self.w(f'float* const ost = reinterpret_cast<float*>(tfb_smem_raw + {self.sm["off_ost"]});')
-      self.w('if (lane == 0 && it > 0) tfb_tc::bulk_wait_read();  // the previous tile\'s copy has read the buffer')
-      self.w('__syncwarp();')
-      self.w('// rows past the tile\'s columns have no place in the buffer')
-      self.open('if (ecol)')
-      self.w('#pragma unroll')
-      self.w(f'for (int i = 0; i < {M // 4}; ++i) reinterpret_cast<float4*>(ost + erow * {M}u)[i] = '
-             'make_float4(acc[4 * i], acc[4 * i + 1], acc[4 * i + 2], acc[4 * i + 3]);')
-      self.close()
-      self.w('tfb_tc::fence_proxy_async();')
-      self.w('__syncwarp();')
-      self.open('if (lane == 0)')
+      orows = self.sm['ost_rows']
       self.w(f'const size_t nrows = (numElements - tile * {te}u) < {te}u ? (numElements - tile * {te}u) * {s.N}u : {te * s.N}u;')
-      self.w('const size_t r0 = equad * 32u;')
-      self.w('const unsigned rows = nrows > r0 ? (unsigned)(nrows - r0 < 32u ? nrows - r0 : 32u) : 0u;')
-      self.w(f'if (rows > 0u) tfb_tc::bulk_store(obase + r0 * {M}u, ost + r0 * {M}u, rows * {M * 4}u);')
-      self.close()
+      for h in range(32 // orows):
+        # rows [r0, r0 + orows) of the warp go through its buffer of orows rows
+        self.w(f'if (lane == 0 && (it > 0{" || true" if h else ""})) tfb_tc::bulk_wait_read();  // the buffer\'s previous copy has read it')
+        self.w('__syncwarp();')
+        self.w('// rows past the tile\'s columns have no place in the buffer')
+        self.open(f'if (ecol && (lane / {orows}u) == {h}u)')
+        self.w(f'float* const orow = ost + (equad * {orows}u + (lane - {h * orows}u)) * {M}u;')
+        self.w('#pragma unroll')
+        self.w(f'for (int i = 0; i < {M // 4}; ++i) reinterpret_cast<float4*>(orow)[i] = '
+               'make_float4(acc[4 * i], acc[4 * i + 1], acc[4 * i + 2], acc[4 * i + 3]);')
+        self.close()
+        self.w('tfb_tc::fence_proxy_async();')
+        self.w('__syncwarp();')
+        self.open('if (lane == 0)')
+        self.w(f'const size_t r0 = equad * 32u + {h * orows}u;')
+        self.w(f'const unsigned rows = nrows > r0 ? (unsigned)(nrows - r0 < {orows}u ? nrows - r0 : {orows}u) : 0u;')
+        self.w(f'if (rows > 0u) tfb_tc::bulk_store(obase + r0 * {M}u, ost + equad * {orows * M}u, rows * {M * 4}u);')
+        self.close()
       self.close()
       self.open('else if (ecol && pel < numElements && (flags == nullptr || flags[pel] != 0u))')
     else:

@@ -118,6 +118,33 @@ def test_chain_o6_one_pass_pipeline(n):
   assert rel <= 1e-6, rel
 
 
+PIPE3_OPTIONS = [{'form': 'u', 'qreg': 1}, {'form': 'u', 'slots': 2}, {'form': 'u', 'loader': 1},
+                 {'form': 'u', 'urows': 2}, {'form': 'u', 'urows': 2, 'fuse': 1}, {'form': 'u', 'qreg': 1, 'fuse': 1},
+                 {'form': 'u', 'urows': 2, 'loader': 2}, {'form': 'u', 'urows': 2, 'fuse': 1, 'loader': 2},
+                 {'form': 'u', 'urows': 1, 'fuse': 0, 'loader': 0}]
+
+
+@pytest.mark.parametrize('variant', PIPE3_OPTIONS, ids=lambda v: ','.join(f'{k}={x}' for k, x in v.items() if k != 'form'))
+@pytest.mark.parametrize('n', [1, 333, 4099])
+def test_warp_specialised_pipeline_options(variant, n):
+  """Options of the warp-specialised pipeline: B rows read into registers a tile ahead,
+  two A slots with two accumulator pairs, a loader warp, two U rows per producer."""
+  got, ref, _, _ = _run('chain_o6', 'tf32x3', n, variant=variant)
+  rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+  assert rel <= 1e-6, rel
+
+
+@pytest.mark.parametrize('variant', PIPE3_OPTIONS[:2] + PIPE3_OPTIONS[4:], ids=lambda v: ','.join(f'{k}={x}' for k, x in v.items() if k != 'form'))
+def test_warp_specialised_pipeline_options_flags_loguniform(variant):
+  got, ref, out, flags = _run('chain_o6', 'tf32x3', 517, use_flags=True, variant=variant)
+  assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-6
+  for e in np.nonzero(flags == 0)[0][:5]:
+    st = out.starts[e]
+    assert np.array_equal(got[st:st + 504], ref[st:st + 504])
+  got, ref, _, _ = _run('chain_o6', 'tf32x3', 777, dist='loguniform', variant=variant)
+  assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-6
+
+
 @pytest.mark.parametrize('case,n', [('chain_o4_q27', 1), ('chain_o4_q27', 77), ('chain_o4_q27', 1001)])
 def test_warp_specialised_pipeline_other_shape(case, n):
   """27 quantities: 4 elements per tile, 24-column A slots, 32-column accumulators."""
