@@ -436,8 +436,12 @@ def extra_workloads(stream, short=False, cpu=True):
     # roofline time of the group: the slower of its FP32-pipe time (nz flops) and HBM time
     g_bound = max(g_nz / fp32, g_bytes / hbm)
     bound_s += g_bound
+    # the same group through its own launcher (the planner's plan for its shape)
+    _, ps = time_launches(lambda i=i: sep[i](**kws[i]), stream, 3, 1)
+    s_ms = sum(ps) / len(ps)
     per_group.append({'basis': b, 'quantities': q, 'elements': n, 'ms': g_ms, 'elements_per_s': n / (g_ms / 1e3),
                       'nz_gflops': g_nz / (g_ms / 1e3) / 1e9,
+                      'standalone_ms': s_ms, 'standalone_plan': gk.gens[i].get_plan().key(),
                       'roofline': {'bound': 'fp32' if g_nz / fp32 >= g_bytes / hbm else 'hbm',
                                    'frac': g_bound / (g_ms / 1e3), 'fp32_frac': g_nz / fp32 / (g_ms / 1e3),
                                    'hbm_frac': g_bytes / hbm / (g_ms / 1e3)}})
@@ -565,8 +569,7 @@ def impl_ours(args, rank, world, dist):
   device = torch.device('cuda', torch.cuda.current_device())
   n = args.elements
   variants = ['plain'] if args.variant == 'plain' else (
-    [args.variant] if args.variant != 'auto' else ['tf32x3', 'plain', 'tf32x3_pipe2', 'tf32x3_form_b', 'tf32x3_form_b2',
-                                                   'tf32x3_form_b_ws'])
+    [args.variant] if args.variant != 'auto' else ['tf32x3', 'plain', 'tf32x3_pipe2'])
   opts_of = {'plain': {}, 'tf32x3': {'precision': 'tf32x3'},
              'tf32x3_ahead': {'precision': 'tf32x3', 'variant': {'form': 'u', 'ahead': 1}},
              'tf32x3_pipe2': {'precision': 'tf32x3', 'variant': {'form': 'u', 'pipe': 2}},

@@ -1276,6 +1276,7 @@ class _TC:
     self.open('else')
     for op in b_ops:
       self._cp_async_copy(op, op.element_volume(), stage_off[op.name], tile_expr, 'stage', 32)
+    self.w('tfb_tc::cp_async_commit();  // wait_group only waits for committed copies')
     self.w('tfb_tc::cp_async_wait_all();')
     self.w('__syncwarp();')
     self.w(f'if (lane == 0) tfb_tc::mbar_arrive(&bars[{BAR_STAGE}]);')

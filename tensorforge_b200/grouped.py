@@ -91,14 +91,15 @@ class GroupedKernel:
     k.append('  extern __shared__ __align__(16) unsigned char tfb_smem_raw[];')
     k.append(f'  {T}* const ubuf = reinterpret_cast<{T}*>(tfb_smem_raw);')
     k.append(f'  {T}* const sA = ubuf + {work_vals};')
-    k.append('  __shared__ unsigned s_item;')
+    k.append('  // the next item is claimed while the current one runs (the atomic\'s latency is hidden)')
+    k.append('  __shared__ unsigned s_item[2];')
+    k.append('  if (threadIdx.x == 0) s_item[0] = atomicAdd(counter, 1u);')
+    k.append('  __syncthreads();')
+    k.append('  unsigned item = s_item[0], nb = 1u;')
     k.append('  int cur = -1;')
     k.append('  for (;;) {')
-    k.append('    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1u);')
-    k.append('    __syncthreads();')
-    k.append('    const unsigned item = s_item;')
-    k.append('    __syncthreads();')
     k.append('    if (item >= num_items) break;')
+    k.append('    if (threadIdx.x == 0) s_item[nb] = atomicAdd(counter, 1u);')
     k.append('    const uint2 wi = items[item];')
     k.append('    if ((int)wi.x != cur) {')
     k.append('      switch (wi.x) {')
@@ -115,6 +116,8 @@ class GroupedKernel:
     k.append('      default: break;')
     k.append('    }')
     k.append('    __syncthreads();')
+    k.append('    item = s_item[nb];')
+    k.append('    nb ^= 1u;')
     k.append('  }')
     k.append('}')
     k.append('')

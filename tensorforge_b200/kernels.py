@@ -19,6 +19,7 @@ EXTRA = [
   ('chain_o4_q27', 'float', {'precision': 'tf32x3'}),
   ('chain_o6', 'float', {'precision': 'tf32x3', 'variant': {'pipe': 1}}),
   ('chain_o6', 'float', {'precision': 'tf32x3', 'variant': {'form': 'u'}}),
+  ('chain_o6', 'float', {'precision': 'tf32x3', 'variant': {'form': 'u', 'pipe': 2}}),
   ('chain_o6', 'float', {'precision': 'tf32x3', 'variant': {'form': 'u', 'ahead': 1}}),
   ('chain_o6', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b'}}),
   ('c0_gemm_ptr', 'float', {'precision': 'tf32x3', 'variant': {'form': 'b'}}),
