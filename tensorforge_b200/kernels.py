@@ -17,6 +17,7 @@ EXTRA = [
   ('chain_o6', 'float', {'precision': 'tf32x3'}),
   ('chain_o6', 'float', {'precision': 'bf16x3'}),
   ('chain_o4_q27', 'float', {'precision': 'tf32x3'}),
+  ('chain_o6_ptr', 'float', {'precision': 'tf32x3'}),
   ('chain_o6', 'float', {'precision': 'tf32x3', 'variant': {'pipe': 1}}),
   ('chain_o6', 'float', {'precision': 'tf32x3', 'variant': {'form': 'u'}}),
   ('chain_o6', 'float', {'precision': 'tf32x3', 'variant': {'form': 'u', 'pipe': 2}}),

@@ -206,6 +206,7 @@ CASES = {
   'chain_o6': (volume_chain, {}, 16),
   'chain_o4_q27': (volume_chain, {'basis': 20, 'quantities': 27, 's_nnz': 72, 'seed': 3}, 16),
   'chain_o3_dense': (volume_chain, {'basis': 10, 'quantities': 9, 'k_density': 1.0, 's_nnz': 81, 'seed': 1, 'terms': 2}, 16),
+  'chain_o6_ptr': (volume_chain, {'q_addr': 'pointer_based', 's_addr': 'pointer_based', 'out_addr': 'pointer_based'}, 16),
   'subbox_0': (subbox_gemm, {'box_a': [0, 0, 33, 9], 'box_b': [0, 0, 9, 11], 'box_c': [0, 0, 33, 11]}, 3),
   'subbox_1': (subbox_gemm, {'box_a': [22, 46, 55, 55], 'box_b': [46, 44, 55, 55], 'box_c': [0, 44, 33, 55]}, 3),
   'subbox_2': (subbox_gemm, {'box_a': [11, 23, 44, 32], 'box_b': [23, 22, 32, 33], 'box_c': [11, 22, 44, 33]}, 3),

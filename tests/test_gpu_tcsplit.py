@@ -145,6 +145,16 @@ def test_warp_specialised_pipeline_options_flags_loguniform(variant):
   assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-6
 
 
+@pytest.mark.parametrize('n', [1, 333, 2001])
+def test_warp_specialised_pipeline_pointer_arrays(n):
+  """Q, S and out through device arrays of element pointers: the B blocks take the copy
+  fallback (no contiguous tile), the output the per-lane stores."""
+  g = __import__('tensorforge_b200.kernels', fromlist=['make']).make('chain_o6_ptr', 'float', precision='tf32x3')
+  assert g.get_plan().params['pipe'] == 3
+  got, ref, _, _ = _run('chain_o6_ptr', 'tf32x3', n)
+  assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-6
+
+
 @pytest.mark.parametrize('case,n', [('chain_o4_q27', 1), ('chain_o4_q27', 77), ('chain_o4_q27', 1001)])
 def test_warp_specialised_pipeline_other_shape(case, n):
   """27 quantities: 4 elements per tile, 24-column A slots, 32-column accumulators."""
