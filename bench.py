@@ -583,6 +583,7 @@ def impl_ours(args, rank, world, dist):
              'tf32x3_qf': {'precision': 'tf32x3', 'variant': {'form': 'u', 'qreg': 1, 'fuse': 1}},
              'tf32x3_u2l': {'precision': 'tf32x3', 'variant': {'form': 'u', 'urows': 2, 'loader': 2}},
              'tf32x3_u2fl': {'precision': 'tf32x3', 'variant': {'form': 'u', 'urows': 2, 'fuse': 1, 'loader': 2}},
+             'tf32x3_nf': {'precision': 'tf32x3', 'variant': {'form': 'u', 'fuse': 0}},
 
              'plain_rs2': {'variant': {'strategy': 'colprog', 'threads': 256, 'rsplit': 2, 'min_blocks': 2}},
              'tf32x3_form_b': {'precision': 'tf32x3', 'variant': {'form': 'b'}},

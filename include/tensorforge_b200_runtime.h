@@ -19,6 +19,12 @@ int tfb_fma_peak_launch(int is_double, void *out, int iters, int blocks, void *s
 // 8 independent m8n8k4 FP64 MMA chains per warp, 8 warps per block, `iters` iterations;
 // flops = 512 * 8 * iters * blocks * 8. `out` holds `blocks` doubles.
 int tfb_dmma_peak_launch(void *out, int iters, int blocks, void *stream);
+// tcgen05 TF32 MMAs of 128 x n x 8 (n = 16..256, multiple of 16) back to back into one
+// accumulator, one CTA of 128 threads per block, A from tensor memory (a_smem = 0) or shared
+// memory (1), B from shared memory; 1 + 8 * floor((iters - 1) / 8) MMAs per CTA, so flops =
+// 2 * 128 * n * 8 * iters * blocks for iters = 8 k + 1. `err` (one device word) is raised to
+// 1 if a CTA's bounded wait for its MMAs runs out.
+int tfb_tc_tf32_peak_launch(int n, int a_smem, unsigned *err, int iters, int blocks, void *stream);
 
 // ---- cost-model MLP, 32 -> 64 -> 64 -> 1 with ReLU, FP32
 // Parameter vector (tfb_mlp_num_params() floats): W1[64][32], b1[64], W2[64][64], b2[64],

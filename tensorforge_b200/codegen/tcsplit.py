@@ -1045,22 +1045,26 @@ class _TC:
       self.w(f'if (!tfb_tc::mbar_wait(&bars[{B["full"]}u + sl], (chunk / {NS}u) & 1u, {lim}ull)) '
              f'{{ ok = false; atomicMax(&tfb_err_{b}, {10 + ti}u); break; }}')
       self.w('tfb_tc::fence_after();')
-      self.open(f'for (int ks = 0; ks < {ksteps}; ++ks)')
-      self.w(f'const unsigned a_hi = tmem + sl * {self.scols}u + ks * {cps}u;')
-      self.w(f'const unsigned a_lo = a_hi + {half}u;')
-      self.w(f'const uint64_t bh = tfb_tc::smem_desc(tfb_tc::smem_u32(tfb_smem_raw + {hi_off}) + ks * 256u, 128u, {sbo}u);')
-      self.w(f'const uint64_t bl = tfb_tc::smem_desc(tfb_tc::smem_u32(tfb_smem_raw + {lo_off}) + ks * 256u, 128u, {sbo}u);')
       first = '(ks > 0) ? 1u : 0u' if ti == 0 else '1u'
+      idesc2 = (idesc & ~(0x3F << 17)) | (((2 * n_mma) >> 3) << 17)
       if self.fuse:
         # B rows [0, N) hi and [N, 2N) lo: one MMA writes main and correction side by side
         assert b_off[ti][1] - b_off[ti][0] == n_mma * kp * es
-        idesc2 = (idesc & ~(0x3F << 17)) | (((2 * n_mma) >> 3) << 17)
-        self.w(f'tfb_tc::{mma}(d_main, a_hi, bh, {idesc2}u, {first});')
-      else:
-        self.w(f'tfb_tc::{mma}(d_main, a_hi, bh, {idesc}u, {first});')
-        self.w(f'tfb_tc::{mma}(d_corr, a_hi, bl, {idesc}u, {first});')
-      self.w(f'tfb_tc::{mma}(d_corr, a_lo, bh, {idesc}u, 1u);')
-      self.close()
+      # all products of a K step before the next step (grouping them by accumulator over the
+      # K steps measured the same: 6.37e8 against 6.35e8 el/s)
+      passes = ([('d_main', 'a_hi', 'bh', idesc2, first)] if self.fuse else
+                [('d_main', 'a_hi', 'bh', idesc, first), ('d_corr', 'a_hi', 'bl', idesc, first)])
+      passes.append(('d_corr', 'a_lo', 'bh', idesc, '1u'))
+      for grp in [passes]:
+        self.open(f'for (int ks = 0; ks < {ksteps}; ++ks)')
+        self.w(f'const unsigned a_hi = tmem + sl * {self.scols}u + ks * {cps}u;')
+        self.w(f'const unsigned a_lo = a_hi + {half}u;')
+        self.w(f'const uint64_t bh = tfb_tc::smem_desc(tfb_tc::smem_u32(tfb_smem_raw + {hi_off}) + ks * 256u, 128u, {sbo}u);')
+        if any(p[2] == 'bl' for p in grp):
+          self.w(f'const uint64_t bl = tfb_tc::smem_desc(tfb_tc::smem_u32(tfb_smem_raw + {lo_off}) + ks * 256u, 128u, {sbo}u);')
+        for d, a, bdesc, idv, acc in grp:
+          self.w(f'tfb_tc::{mma}({d}, {a}, {bdesc}, {idv}u, {acc});')
+        self.close()
       self.w(f'tfb_tc::mma_commit(&bars[{B["free"]}u + sl]);')
       self.w('++chunk;')
       self.w('}')

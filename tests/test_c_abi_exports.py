@@ -42,7 +42,7 @@ def test_runtime_library_exports_its_headers():
     for name in names:
       assert hasattr(lib, name), f'{name} ({header}) not exported by {native.LIB}'
       checked += 1
-  assert checked == 10  # 8 runtime entry points + 2 status helpers
+  assert checked == 11  # 9 runtime entry points + 2 status helpers
 
 
 def test_headers_are_all_covered():
