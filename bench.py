@@ -584,6 +584,7 @@ def impl_ours(args, rank, world, dist):
              'tf32x3_u2l': {'precision': 'tf32x3', 'variant': {'form': 'u', 'urows': 2, 'loader': 2}},
              'tf32x3_u2fl': {'precision': 'tf32x3', 'variant': {'form': 'u', 'urows': 2, 'fuse': 1, 'loader': 2}},
              'tf32x3_nf': {'precision': 'tf32x3', 'variant': {'form': 'u', 'fuse': 0}},
+             'tf32x3_l3': {'precision': 'tf32x3', 'variant': {'form': 'u', 'loader': 3}},
 
              'plain_rs2': {'variant': {'strategy': 'colprog', 'threads': 256, 'rsplit': 2, 'min_blocks': 2}},
              'tf32x3_form_b': {'precision': 'tf32x3', 'variant': {'form': 'b'}},

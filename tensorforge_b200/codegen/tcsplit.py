@@ -146,7 +146,7 @@ def smem_plan_v2(shape, precision):
               pitch=pitch, ubuf_bytes=ubuf, off_bar=off_bar, total=total, te=te, tc=tc)
 
 
-def smem_plan_v3(shape, precision, qreg=False, fuse=False):
+def smem_plan_v3(shape, precision, qreg=False, fuse=False, rbuf2=False):
   """Shared memory of the warp-specialised pipeline: the one-pass layout, an output staging
   buffer for the epilogue warps' bulk stores (32 rows per warp, or 16 rows at a time when
   only that fits) and the B operand. Without `fuse` B is stored for the real output rows
@@ -172,6 +172,16 @@ def smem_plan_v3(shape, precision, qreg=False, fuse=False):
   out = dict(sm, rows_b=rows_b, b_bytes=b_bytes, ost_rows=0)
   for k in ('off_stage', 'off_u', 'off_bar', 'total'):
     out[k] = sm[k] - shift
+  if rbuf2:
+    # a second buffer for the R blocks (the loader fetches them one tile ahead)
+    rstart = min(sm['stage_off'][op.name] for op in sm['r_ops'])
+    rend = max(sm['stage_off'][op.name] + sm['te'] * _pad(op.storage_size() if op.sparse else op.element_volume(), 4)
+               for op in sm['r_ops'])
+    rbytes = _pad((rend - rstart) * 4, 128)
+    out['off_rbuf1'] = out['off_bar']
+    out['rbuf_delta'] = (out['off_rbuf1'] - out['off_stage']) // 4 - rstart
+    out['off_bar'] += rbytes
+    out['total'] += rbytes
   if shape.M % 4 == 0:
     for rows in (32, 16):
       ost = _pad(4 * rows * shape.M * 4, 128)
@@ -248,7 +258,8 @@ def plan(chain, shape, precision, variant):
     # products as one MMA of twice the width when the whole B tiles fit
     qreg = bool(int(variant.get('qreg', 0)))
     fuse = int(variant.get('fuse', 1 if smem_plan_v3(shape, precision, qreg, True)['total'] <= _plan.SMEM_LIMIT else 0))
-  sm = ((lambda sh, pr: smem_plan_v3(sh, pr, bool(int(variant.get('qreg', 0))), bool(fuse)))
+  rbuf2 = pipe == 3 and int(variant.get('loader', 2)) == 3 and not int(variant.get('qreg', 0))
+  sm = ((lambda sh, pr: smem_plan_v3(sh, pr, bool(int(variant.get('qreg', 0))), bool(fuse), rbuf2))
         if pipe == 3 else smem_plan_v2)(shape, precision) if pipe in (2, 3) else None
   if sm is None or sm['total'] > _plan.SMEM_LIMIT:
     pipe = 1
@@ -276,6 +287,8 @@ def plan(chain, shape, precision, variant):
     # the small R copies; 1 fetches all inputs (measured slower: 4.8e8 el/s, the stage is
     # single-buffered and one warp issues the R copies slowly); 0 none
     params['loader'] = int(variant.get('loader', 2))
+    if params['loader'] == 3 and int(variant.get('qreg', 0)):
+      params['loader'] = 2
     # option: the per-element B operand goes straight from global memory into registers one
     # tile ahead (two rows per producer), so the stage only holds the R blocks
     b_ops = {id(t.B) for t in shape.terms}
@@ -440,7 +453,8 @@ class _TC:
     self.pipe = plan_.params.get('pipe', 1)
     self.qreg = self.pipe == 3 and int(plan_.params.get('qreg', 0)) == 1
     self.fuse = self.pipe == 3 and int(plan_.params.get('fuse', 0)) == 1
-    self.sm = (smem_plan_v3(shape, self.prec, self.qreg, self.fuse) if self.pipe == 3 else
+    self.rbuf2 = self.pipe == 3 and int(plan_.params.get('loader', 0)) == 3 and not self.qreg
+    self.sm = (smem_plan_v3(shape, self.prec, self.qreg, self.fuse, self.rbuf2) if self.pipe == 3 else
                smem_plan_v2(shape, self.prec) if self.pipe == 2 else smem_plan(shape, self.prec))
     self.LC = plan_.params['chunk']
     self.ahead = bool(plan_.params.get('ahead', 0))
@@ -556,7 +570,7 @@ class _TC:
     # loader warp: 1 fetches all inputs of the next tile, 2 only the bulk copy of the B
     # blocks (the producers keep issuing the small R copies)
     self.loader_mode = int(self.plan.params.get('loader', 0)) if p3 else 0
-    self.loader = self.loader_mode in (1, 2)
+    self.loader = self.loader_mode in (1, 2, 3)
     nthreads = 32 * (4 * H + 1 + (4 if p3 else 0) + (1 if self.loader else 0))
     BAR_FULL, BAR_FREE, BAR_DFULL, BAR_DFREE = 0, nterms, 2 * nterms, 2 * nterms + 1
     if p3:
@@ -571,13 +585,14 @@ class _TC:
       BAR_FULL, BAR_FREE = 0, self.NS
       BAR_DFULL, BAR_DFREE = 2 * self.NS, 2 * self.NS + self.ND
       self.BAR = dict(full=BAR_FULL, free=BAR_FREE, dfull=BAR_DFULL, dfree=BAR_DFREE,
-                      stage=2 * self.NS + 2 * self.ND, sfree=2 * self.NS + 2 * self.ND + 1)
+                      stage=2 * self.NS + 2 * self.ND, sfree=2 * self.NS + 2 * self.ND + 1,
+                      rstage=2 * self.NS + 2 * self.ND + 2)
 
     self.w(f'__global__ void __launch_bounds__({nthreads}, 1) {kname}({", ".join(self.params(globals_))}) {{')
     self.ind += 1
     self.w('extern __shared__ __align__(1024) unsigned char tfb_smem_raw[];')
     self.w(f'uint64_t* const bars = reinterpret_cast<uint64_t*>(tfb_smem_raw + {sm["off_bar"]});')
-    nbars = (2 * self.NS + 2 * self.ND + 2) if p3 else 2 * nterms + (3 if self.pipe == 2 else 2)
+    nbars = (2 * self.NS + 2 * self.ND + 2 + (2 if self.rbuf2 else 0)) if p3 else 2 * nterms + (3 if self.pipe == 2 else 2)
     BAR_STAGE = self.BAR['stage'] if p3 else 2 * nterms + 2
     self.w(f'unsigned* const tmem_slot = reinterpret_cast<unsigned*>(bars + {nbars});')
     probe = int(self.plan.params.get('wait_probe', 0))
@@ -634,7 +649,11 @@ class _TC:
       self.w(f'tfb_tc::mbar_init(&bars[{BAR_DFREE}], {NP}u);')
     if self.pipe in (2, 3):
       # one arrival per copying thread (cp.async completion) + the bulk-copy issuer's expect_tx
-      self.w(f'tfb_tc::mbar_init(&bars[{BAR_STAGE}], {(32 if self.loader_mode == 1 else NP) + 1}u);')
+      stage_count = {1: 32 + 1, 3: 1}.get(self.loader_mode, NP + 1)
+      self.w(f'tfb_tc::mbar_init(&bars[{BAR_STAGE}], {stage_count}u);')
+      if self.rbuf2:
+        for i in range(2):
+          self.w(f'tfb_tc::mbar_init(&bars[{self.BAR["rstage"] + i}], 32u);')
     if probe:
       self.w('tfb_tc::mbar_init(probe_bar, 1u);')
     self.w('asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");')
@@ -927,7 +946,8 @@ class _TC:
           continue
         nr = t.R.storage_size()
         self.open('')
-        self.w(f'const float4* const rq = reinterpret_cast<const float4*>(stage + {stage_off[t.R.name]} + ei * {_pad(nr, 4)}u);')
+        rbase = 'rstage' if getattr(self, 'rbuf2', False) else 'stage'
+        self.w(f'const float4* const rq = reinterpret_cast<const float4*>({rbase} + {stage_off[t.R.name]} + ei * {_pad(nr, 4)}u);')
         for v in range((nr + 3) // 4):
           self.w(f'const float4 r{v} = rq[{v}];')
         look = t.R.sparse_lookup() if t.R.sparse else None
@@ -1130,7 +1150,7 @@ class _TC:
     self.w('unsigned it = 0;')
     if self.qreg:
       self._q_decl()
-    rcopies = self.loader_mode != 1   # the producers copy the R blocks
+    rcopies = self.loader_mode not in (1, 3)   # the producers copy the R blocks
     if rcopies:
       self.w('bool pending = false;')
       self.open('if (blockIdx.x < numTiles)')
@@ -1150,6 +1170,10 @@ class _TC:
     self.w('// stops all producers at the next tile boundary (a barrier-wide OR), never mid-tile')
     self.w(f'if (tfb_tc::any_sync(1, {NP}, !ok)) break;')
     self.w(f'if (!tfb_tc::mbar_wait(&bars[{BAR_STAGE}], it & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 40u); }}')
+    if self.rbuf2:
+      self.w(f'if (!tfb_tc::mbar_wait(&bars[{self.BAR["rstage"]}u + (it & 1u)], (it >> 1) & 1u, {lim}ull)) '
+             f'{{ ok = false; atomicMax(&tfb_err_{b}, 43u); }}')
+      self.w(f'const float* const rstage = stage + ((it & 1u) ? {self.sm["rbuf_delta"]} : 0);')
     if rcopies:
       self.w('const size_t ntile = tile + gridDim.x;')
       self.w('const bool has_next = ntile < numTiles;')
@@ -1287,15 +1311,33 @@ class _TC:
     self.close()
     self.close()
 
+  def _r_copies(self, tile_expr, buf_expr, stage_off):
+    """Loader mode 3: the R blocks of a tile into R buffer `buf_expr` (0 or 1) by the 32 lanes,
+    each lane's copies counted on that buffer's mbarrier, then committed as one group."""
+    self.open('')
+    self.w(f'float* const rdst = stage + (({buf_expr}) ? {self.sm["rbuf_delta"]} : 0);')
+    for op in self.sm['r_ops']:
+      vals = op.storage_size() if op.sparse else op.element_volume()
+      self._cp_async_copy(op, vals, stage_off[op.name], tile_expr, 'rdst', 32)
+    self.w(f'tfb_tc::cp_async_mbar_arrive(&bars[{self.BAR["rstage"]}u + (({buf_expr}) ? 1u : 0u)]);')
+    self.w('tfb_tc::cp_async_commit();')
+    self.close()
+
   def _loader_v3(self, stage_off, lim, BAR_STAGE):
-    """Loader warp: fetches each tile's inputs into the stage (bulk copy of the B blocks by
-    lane 0, cp.async of the R blocks by the 32 lanes) as soon as the producers have released
-    it, so the producers never issue copies themselves."""
+    """Loader warp: fetches the inputs of the next tile into the stage as soon as the
+    producers have released it. Mode 1: B and R blocks; mode 2: the bulk copy of the B
+    blocks only (the producers copy R); mode 3: the B blocks, and the R blocks one tile
+    further ahead into two alternating R buffers, so the producers issue no copies."""
     b = self.base
     self.open('else')
     self.w('const unsigned ptid = lane;')
     self.w('unsigned it = 0;')
     self.w('bool pending = false;')
+    if self.loader_mode == 3:
+      self._r_copies('(size_t)blockIdx.x', '0u', stage_off)
+      self.open('if ((size_t)blockIdx.x + gridDim.x < numTiles)')
+      self._r_copies('(size_t)blockIdx.x + gridDim.x', '1u', stage_off)
+      self.close()
     self.open('for (size_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++it)')
     self.w(f'if (it > 0u && !tfb_tc::mbar_wait(&bars[{self.BAR["sfree"]}], (it - 1u) & 1u, {lim}ull)) '
            f'{{ ok = false; atomicMax(&tfb_err_{b}, 42u); break; }}')
@@ -1304,6 +1346,11 @@ class _TC:
       self._loads_v2('tile', 2, stage_off, BAR_STAGE, 32, sync=False)
     else:
       self._bulk_b_only('tile', stage_off, BAR_STAGE)
+    if self.loader_mode == 3:
+      # R of tile it + 1 into the buffer tile it - 1 has released
+      self.open('if (it > 0u && tile + gridDim.x < numTiles)')
+      self._r_copies('tile + gridDim.x', '(it + 1u) & 1u', stage_off)
+      self.close()
     self.w('pending = true;')
     self.close()
     self.w('// copies still in flight must land before the CTA exits: the last tile\'s, consumed')

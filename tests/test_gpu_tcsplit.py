@@ -121,8 +121,8 @@ def test_chain_o6_one_pass_pipeline(n):
 PIPE3_OPTIONS = [{'form': 'u', 'qreg': 1}, {'form': 'u', 'slots': 2}, {'form': 'u', 'loader': 1},
                  {'form': 'u', 'urows': 2}, {'form': 'u', 'urows': 2, 'fuse': 1}, {'form': 'u', 'qreg': 1, 'fuse': 1},
                  {'form': 'u', 'urows': 2, 'loader': 2}, {'form': 'u', 'urows': 2, 'fuse': 1, 'loader': 2},
-                 {'form': 'u', 'urows': 1, 'fuse': 0, 'loader': 0}',
-                 {'form': 'u', 'fuse': 0}]
+                 {'form': 'u', 'urows': 1, 'fuse': 0, 'loader': 0},
+                 {'form': 'u', 'fuse': 0}, {'form': 'u', 'loader': 3}]
 
 
 @pytest.mark.parametrize('variant', PIPE3_OPTIONS, ids=lambda v: ','.join(f'{k}={x}' for k, x in v.items() if k != 'form'))
