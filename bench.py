@@ -585,6 +585,11 @@ def impl_ours(args, rank, world, dist):
              'tf32x3_u2fl': {'precision': 'tf32x3', 'variant': {'form': 'u', 'urows': 2, 'fuse': 1, 'loader': 2}},
              'tf32x3_nf': {'precision': 'tf32x3', 'variant': {'form': 'u', 'fuse': 0}},
              'tf32x3_l3': {'precision': 'tf32x3', 'variant': {'form': 'u', 'loader': 3}},
+             'tf32x3_spin': {'precision': 'tf32x3', 'variant': {'form': 'u', 'sleep': 0}},
+             'tf32x3_ds': {'precision': 'tf32x3', 'variant': {'form': 'u', 'ostage': 0}},
+             'tf32x3_op': {'precision': 'tf32x3', 'variant': {'form': 'u', 'opad': 1}},
+             'tf32x3_uw': {'precision': 'tf32x3', 'variant': {'form': 'u', 'uwarp': 1}},
+             'tf32x3_opuw': {'precision': 'tf32x3', 'variant': {'form': 'u', 'opad': 1, 'uwarp': 1}},
 
              'plain_rs2': {'variant': {'strategy': 'colprog', 'threads': 256, 'rsplit': 2, 'min_blocks': 2}},
              'tf32x3_form_b': {'precision': 'tf32x3', 'variant': {'form': 'b'}},

@@ -146,7 +146,7 @@ def smem_plan_v2(shape, precision):
               pitch=pitch, ubuf_bytes=ubuf, off_bar=off_bar, total=total, te=te, tc=tc)
 
 
-def smem_plan_v3(shape, precision, qreg=False, fuse=False, rbuf2=False):
+def smem_plan_v3(shape, precision, qreg=False, fuse=False, rbuf2=False, opad=False):
   """Shared memory of the warp-specialised pipeline: the one-pass layout, an output staging
   buffer for the epilogue warps' bulk stores (32 rows per warp, or 16 rows at a time when
   only that fits) and the B operand. Without `fuse` B is stored for the real output rows
@@ -183,8 +183,9 @@ def smem_plan_v3(shape, precision, qreg=False, fuse=False, rbuf2=False):
     out['off_bar'] += rbytes
     out['total'] += rbytes
   if shape.M % 4 == 0:
+    out['ost_pitch'] = shape.M + 4 if opad else shape.M
     for rows in (32, 16):
-      ost = _pad(4 * rows * shape.M * 4, 128)
+      ost = _pad(4 * rows * out['ost_pitch'] * 4, 128)
       if out['total'] + ost <= _plan.SMEM_LIMIT:
         out['off_ost'] = out['off_bar']
         out['off_bar'] += ost
@@ -258,8 +259,14 @@ def plan(chain, shape, precision, variant):
     # products as one MMA of twice the width when the whole B tiles fit
     qreg = bool(int(variant.get('qreg', 0)))
     fuse = int(variant.get('fuse', 1 if smem_plan_v3(shape, precision, qreg, True)['total'] <= _plan.SMEM_LIMIT else 0))
-  rbuf2 = pipe == 3 and int(variant.get('loader', 2)) == 3 and not int(variant.get('qreg', 0))
-  sm = ((lambda sh, pr: smem_plan_v3(sh, pr, bool(int(variant.get('qreg', 0))), bool(fuse), rbuf2))
+  # loader warp default: 3 (B blocks and the next tile's R blocks) when the second R buffer
+  # fits, else 2
+  rbuf2_fits = (pipe == 3 and not int(variant.get('qreg', 0))
+                and smem_plan_v3(shape, precision, False, bool(fuse), True)['total'] <= _plan.SMEM_LIMIT)
+  loader_default = 3 if rbuf2_fits else 2
+  rbuf2 = rbuf2_fits and int(variant.get('loader', loader_default)) == 3
+  opad = pipe == 3 and bool(int(variant.get('opad', 0)))
+  sm = ((lambda sh, pr: smem_plan_v3(sh, pr, bool(int(variant.get('qreg', 0))), bool(fuse), rbuf2, opad))
         if pipe == 3 else smem_plan_v2)(shape, precision) if pipe in (2, 3) else None
   if sm is None or sm['total'] > _plan.SMEM_LIMIT:
     pipe = 1
@@ -283,11 +290,13 @@ def plan(chain, shape, precision, variant):
     if ns not in (2, nt) or ns * scols + (1 if ns == nt else 2) * dcols > 512:
       ns = 2
     params['slots'] = ns
-    # loader warp: 2 (default) issues only the bulk copy of the B blocks, the producers keep
-    # the small R copies; 1 fetches all inputs (measured slower: 4.8e8 el/s, the stage is
-    # single-buffered and one warp issues the R copies slowly); 0 none
-    params['loader'] = int(variant.get('loader', 2))
-    if params['loader'] == 3 and int(variant.get('qreg', 0)):
+    # loader warp: 3 (default) issues the bulk copy of the B blocks and fetches the R blocks
+    # of the next tile into the other of two R buffers (order-6 chain, 500,000 elements:
+    # 6.44e8 el/s against 6.36e8 with mode 2); 2 issues only the bulk copy of the B blocks,
+    # the producers keep the small R copies; 1 fetches all inputs into the one stage
+    # (measured slower: 4.8e8 el/s, one warp issues the R copies slowly); 0 none
+    params['loader'] = int(variant.get('loader', loader_default))
+    if params['loader'] == 3 and not rbuf2:
       params['loader'] = 2
     # option: the per-element B operand goes straight from global memory into registers one
     # tile ahead (two rows per producer), so the stage only holds the R blocks
@@ -303,6 +312,21 @@ def plan(chain, shape, precision, variant):
     params['fuse'] = 1
   if int(variant.get('urows', 2 if pipe == 3 else 1)) == 2 and pipe in (2, 3) and all(t.K % 2 == 0 for t in shape.terms):
     params['urows'] = 2
+  if pipe == 3 and int(variant.get('sleep', 1)):
+    # waiting threads sleep in try_wait (global-timer bound) instead of spinning, leaving
+    # the issue slots to the producers (order-6 chain, 500,000 elements: 6.51e8 el/s
+    # against 6.45e8 with spinning waits)
+    params['sleep'] = 1
+  if opad:
+    # option: output staging rows padded by 16 bytes (no bank conflicts on the staging
+    # stores), each row written by its own bulk copy
+    params['opad'] = 1
+  if pipe == 3 and int(variant.get('uwarp', 0)):
+    # option: U pass work items aligned to warps (no warp straddles two elements)
+    params['uwarp'] = 1
+  if pipe == 3 and not int(variant.get('ostage', 1)):
+    # option: the epilogue warps store their columns straight from registers (no staging)
+    params['ostage'] = 0
   if int(variant.get('wait_probe', 0)) > 0:
     # failure-detection check: the kernel first waits, with this many polls, on an mbarrier
     # that nothing arrives on, records error 30 and returns before issuing any copy or MMA
@@ -335,6 +359,24 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsign
     if (ok) return true;
   }
   return false;
+}
+// bounded wait on phase `parity` that lets the thread sleep inside try_wait (the suspend-time
+// hint, in ns) until the phase completes, so a waiting warp issues few instructions; returns
+// false once `limit_ns` nanoseconds of the global timer have passed since the first poll
+__device__ __forceinline__ bool mbar_wait_s(uint64_t* bar, unsigned parity, unsigned long long limit_ns) {
+  const unsigned addr = smem_u32(bar);
+  const unsigned hint_ns = 1000000u;
+  unsigned long long t0 = 0;
+  for (;;) {
+    unsigned ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok) : "r"(addr), "r"(parity), "r"(hint_ns) : "memory");
+    if (ok) return true;
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (t0 == 0) t0 = t;
+    else if (t - t0 > limit_ns) return false;
+  }
 }
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -440,7 +482,8 @@ def emit_tcsplit(chain, plan_, context, base_name, globals_):
 
 
 class _TC:
-  WAIT_LIMIT = 1 << 26
+  WAIT_LIMIT = 1 << 26         # polls of a spinning wait
+  WAIT_NS = 2000000000         # nanoseconds of a sleeping wait
 
   def __init__(self, chain, shape, plan_, ctx, base):
     self.chain = chain
@@ -454,7 +497,8 @@ class _TC:
     self.qreg = self.pipe == 3 and int(plan_.params.get('qreg', 0)) == 1
     self.fuse = self.pipe == 3 and int(plan_.params.get('fuse', 0)) == 1
     self.rbuf2 = self.pipe == 3 and int(plan_.params.get('loader', 0)) == 3 and not self.qreg
-    self.sm = (smem_plan_v3(shape, self.prec, self.qreg, self.fuse, self.rbuf2) if self.pipe == 3 else
+    self.opad = self.pipe == 3 and bool(int(plan_.params.get('opad', 0)))
+    self.sm = (smem_plan_v3(shape, self.prec, self.qreg, self.fuse, self.rbuf2, self.opad) if self.pipe == 3 else
                smem_plan_v2(shape, self.prec) if self.pipe == 2 else smem_plan(shape, self.prec))
     self.LC = plan_.params['chunk']
     self.ahead = bool(plan_.params.get('ahead', 0))
@@ -565,8 +609,11 @@ class _TC:
       slot_base.append(col)
       col += lay['slot_cols'][ti]
     d_main, d_corr = col, col + n_mma
-    lim = self.WAIT_LIMIT
     p3 = self.pipe == 3
+    # waits that sleep in try_wait (bounded by the global timer) or spin (bounded by polls)
+    sleep = p3 and bool(int(self.plan.params.get('sleep', 0)))
+    self.wfn = 'mbar_wait_s' if sleep else 'mbar_wait'
+    lim = self.WAIT_NS if sleep else self.WAIT_LIMIT
     # loader warp: 1 fetches all inputs of the next tile, 2 only the bulk copy of the B
     # blocks (the producers keep issuing the small R copies)
     self.loader_mode = int(self.plan.params.get('loader', 0)) if p3 else 0
@@ -680,7 +727,7 @@ class _TC:
       self.open('if (lane == 0)')
       self.w('unsigned it = 0;')
       self.open('for (size_t tile = blockIdx.x; tile < numTiles && ok; tile += gridDim.x, ++it)')
-      self.w(f'if (it > 0 && !tfb_tc::mbar_wait(&bars[{BAR_DFREE}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 13u); break; }}')
+      self.w(f'if (it > 0 && !tfb_tc::{self.wfn}(&bars[{BAR_DFREE}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 13u); break; }}')
       mma = 'mma_tf32' if prec == 'tf32x3' else 'mma_f16'
       for ti, t in enumerate(s.terms):
         kp = lay['kpad'][ti]
@@ -689,7 +736,7 @@ class _TC:
         sbo = (kp // ke) * 128
         acols = lay['a_cols'][ti]
         cps = lay['ks'] * es // 4
-        self.w(f'if (!tfb_tc::mbar_wait(&bars[{BAR_FULL + ti}], it & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, {10 + ti}u); break; }}')
+        self.w(f'if (!tfb_tc::{self.wfn}(&bars[{BAR_FULL + ti}], it & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, {10 + ti}u); break; }}')
         self.w('tfb_tc::fence_after();')
         self.open(f'for (int ks = 0; ks < {ksteps}; ++ks)')
         self.w(f'const unsigned a_hi = tmem + {slot_base[ti]}u + ks * {cps}u;')
@@ -751,7 +798,7 @@ class _TC:
       self.close()
       # epilogue of the previous tile
       self.open('if (have_prev)')
-      self.w(f'if (!tfb_tc::mbar_wait(&bars[{BAR_DFULL}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 20u); }}')
+      self.w(f'if (!tfb_tc::{self.wfn}(&bars[{BAR_DFULL}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 20u); }}')
       self.w('tfb_tc::fence_after();')
       self._epilogue(d_main, d_corr, NP)
       self.close()
@@ -922,7 +969,24 @@ class _TC:
       terms = [(ti, t) for ti, t in enumerate(s.terms) if t.B is B]
       K, P = terms[0][1].K, terms[0][1].P
       bvals = _pad(B.element_volume(), 4)
-      if two:
+      ipe = K // 2 if two else K   # work items (rows or row pairs) per element
+      if int(self.plan.params.get('uwarp', 0)) and ipe <= 32 and NP % 32 == 0:
+        # warp-aligned items: a warp takes 32 // ipe whole elements (lanes past them idle),
+        # so no warp's loads and stores straddle two elements' rows (one bank wavefront
+        # fewer per access when ipe does not divide 32)
+        epw = 32 // ipe
+        self.w(f'const unsigned usub = lane / {ipe}u, uidx = lane - usub * {ipe}u;')
+        self.open(f'for (unsigned ew = (ptid >> 5) * {epw}u + usub; ew < {_pad(te, epw)}u; ew += {NP // 32 * epw}u)')
+        self.w(f'if (usub >= {epw}u || ew >= {te}u) continue;')
+        self.w('const unsigned ei = ew;')
+        self.w(f'const unsigned l = {"2u * uidx" if two else "uidx"};')
+        if two:
+          assert K % 2 == 0 and pitch % 2 == 0 and stage_off[B.name] % 2 == 0
+        self.w(f'const float* const bq = stage + {stage_off[B.name]} + ei * {bvals}u + l;')
+        for m in range(P):
+          self.w(f'const float2 q{m} = *reinterpret_cast<const float2*>(bq + {m * K});' if two
+                 else f'const float q{m} = bq[{m * K}];')
+      elif two:
         assert K % 2 == 0 and pitch % 2 == 0 and stage_off[B.name] % 2 == 0
         self.open(f'for (unsigned q = ptid; q < {te * K // 2}u; q += {NP}u)')
         self.w(f'const unsigned ei = q / {K // 2}u, l = 2u * (q - ei * {K // 2}u);')
@@ -997,7 +1061,7 @@ class _TC:
     self.w('const size_t ntile = tile + gridDim.x;')
     self.w('const bool has_next = more && ntile < numTiles;')
     self.open('if (more)')
-    self.w(f'if (!tfb_tc::mbar_wait(&bars[{BAR_STAGE}], it & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 40u); }}')
+    self.w(f'if (!tfb_tc::{self.wfn}(&bars[{BAR_STAGE}], it & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 40u); }}')
     self.w('pending = false;')
     self._u_phase_v2(stage_off, NP)
     self.close()
@@ -1006,7 +1070,7 @@ class _TC:
     self._loads_v2('ntile', 1, stage_off, BAR_STAGE, NP)
     self.close()
     self.open('if (have_prev)')
-    self.w(f'if (!tfb_tc::mbar_wait(&bars[{BAR_DFULL}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 20u); }}')
+    self.w(f'if (!tfb_tc::{self.wfn}(&bars[{BAR_DFULL}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 20u); }}')
     self.w('tfb_tc::fence_after();')
     self._epilogue(d_main, d_corr, NP, sbuf='stage', final_sync=False)
     self.close()
@@ -1029,7 +1093,7 @@ class _TC:
     self.w('prev_tile = tile; have_prev = true;')
     self.close()
     self.w('// a stage load still in flight after an abort must land before the CTA exits')
-    self.w(f'if (pending && !tfb_tc::mbar_wait(&bars[{BAR_STAGE}], it & 1u, {lim}ull)) atomicMax(&tfb_err_{b}, 41u);')
+    self.w(f'if (pending && !tfb_tc::{self.wfn}(&bars[{BAR_STAGE}], it & 1u, {lim}ull)) atomicMax(&tfb_err_{b}, 41u);')
     self.w('tfb_tc::cp_async_wait_all();')
     self.w('if (ptid == 0) tfb_tc::bulk_wait();')
     self.close()
@@ -1051,7 +1115,7 @@ class _TC:
     self.open('for (size_t tile = blockIdx.x; tile < numTiles && ok; tile += gridDim.x, ++it)')
     self.w(f'const unsigned db = it % {ND}u;')
     self.w(f'const unsigned d_main = tmem + {self.d_base}u + db * {self.dcols}u, d_corr = d_main + {n_mma}u;')
-    self.w(f'if (it >= {ND}u && !tfb_tc::mbar_wait(&bars[{B["dfree"]}u + db], ((it - {ND}u) / {ND}u) & 1u, {lim}ull)) '
+    self.w(f'if (it >= {ND}u && !tfb_tc::{self.wfn}(&bars[{B["dfree"]}u + db], ((it - {ND}u) / {ND}u) & 1u, {lim}ull)) '
            f'{{ ok = false; atomicMax(&tfb_err_{b}, 13u); break; }}')
     self.w('tfb_tc::fence_after();')
     for ti, t in enumerate(s.terms):
@@ -1062,7 +1126,7 @@ class _TC:
       cps = lay['ks'] * es // 4
       self.w('{')
       self.w(f'const unsigned sl = chunk % {NS}u;')
-      self.w(f'if (!tfb_tc::mbar_wait(&bars[{B["full"]}u + sl], (chunk / {NS}u) & 1u, {lim}ull)) '
+      self.w(f'if (!tfb_tc::{self.wfn}(&bars[{B["full"]}u + sl], (chunk / {NS}u) & 1u, {lim}ull)) '
              f'{{ ok = false; atomicMax(&tfb_err_{b}, {10 + ti}u); break; }}')
       self.w('tfb_tc::fence_after();')
       first = '(ks > 0) ? 1u : 0u' if ti == 0 else '1u'
@@ -1102,7 +1166,7 @@ class _TC:
     half = self.scols // 2
     self.open('')
     self.w(f'const unsigned chunk = it * {nterms}u + {ti}u, sl = chunk % {NS}u;')
-    self.w(f'if (chunk >= {NS}u && !tfb_tc::mbar_wait(&bars[{B["free"]}u + sl], ((chunk - {NS}u) / {NS}u) & 1u, {lim}ull)) '
+    self.w(f'if (chunk >= {NS}u && !tfb_tc::{self.wfn}(&bars[{B["free"]}u + sl], ((chunk - {NS}u) / {NS}u) & 1u, {lim}ull)) '
            f'{{ ok = false; atomicMax(&tfb_err_{b}, {30 + ti}u); }}')
     self.w('tfb_tc::fence_after();')
     self.w(f'const unsigned slot = lane_addr + sl * {self.scols}u;')
@@ -1169,9 +1233,9 @@ class _TC:
     self.w('// every producer takes the same branches around named barriers: a timeout anywhere')
     self.w('// stops all producers at the next tile boundary (a barrier-wide OR), never mid-tile')
     self.w(f'if (tfb_tc::any_sync(1, {NP}, !ok)) break;')
-    self.w(f'if (!tfb_tc::mbar_wait(&bars[{BAR_STAGE}], it & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 40u); }}')
+    self.w(f'if (!tfb_tc::{self.wfn}(&bars[{BAR_STAGE}], it & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 40u); }}')
     if self.rbuf2:
-      self.w(f'if (!tfb_tc::mbar_wait(&bars[{self.BAR["rstage"]}u + (it & 1u)], (it >> 1) & 1u, {lim}ull)) '
+      self.w(f'if (!tfb_tc::{self.wfn}(&bars[{self.BAR["rstage"]}u + (it & 1u)], (it >> 1) & 1u, {lim}ull)) '
              f'{{ ok = false; atomicMax(&tfb_err_{b}, 43u); }}')
       self.w(f'const float* const rstage = stage + ((it & 1u) ? {self.sm["rbuf_delta"]} : 0);')
     if rcopies:
@@ -1207,7 +1271,7 @@ class _TC:
     self.close()
     if rcopies:
       self.w('// a stage load still in flight after an abort must land before the CTA exits')
-      self.w(f'if (pending && !tfb_tc::mbar_wait(&bars[{BAR_STAGE}], it & 1u, {lim}ull)) atomicMax(&tfb_err_{b}, 41u);')
+      self.w(f'if (pending && !tfb_tc::{self.wfn}(&bars[{BAR_STAGE}], it & 1u, {lim}ull)) atomicMax(&tfb_err_{b}, 41u);')
       self.w('tfb_tc::cp_async_wait_all();')
       self.w('if (ptid == 0) tfb_tc::bulk_wait();')
     self.close()
@@ -1339,7 +1403,7 @@ class _TC:
       self._r_copies('(size_t)blockIdx.x + gridDim.x', '1u', stage_off)
       self.close()
     self.open('for (size_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++it)')
-    self.w(f'if (it > 0u && !tfb_tc::mbar_wait(&bars[{self.BAR["sfree"]}], (it - 1u) & 1u, {lim}ull)) '
+    self.w(f'if (it > 0u && !tfb_tc::{self.wfn}(&bars[{self.BAR["sfree"]}], (it - 1u) & 1u, {lim}ull)) '
            f'{{ ok = false; atomicMax(&tfb_err_{b}, 42u); break; }}')
     if self.loader_mode == 1:
       self._loads_v2('tile', 1, stage_off, BAR_STAGE, 32)
@@ -1355,7 +1419,7 @@ class _TC:
     self.close()
     self.w('// copies still in flight must land before the CTA exits: the last tile\'s, consumed')
     self.w('// by the producers, or one nobody consumed after an abort')
-    self.w(f'if (pending && !tfb_tc::mbar_wait(&bars[{BAR_STAGE}], (it - 1u) & 1u, {lim}ull)) atomicMax(&tfb_err_{b}, 41u);')
+    self.w(f'if (pending && !tfb_tc::{self.wfn}(&bars[{BAR_STAGE}], (it - 1u) & 1u, {lim}ull)) atomicMax(&tfb_err_{b}, 41u);')
     self.w('tfb_tc::cp_async_wait_all();')
     self.w('if (lane == 0) tfb_tc::bulk_wait();')
     self.close()
@@ -1377,7 +1441,7 @@ class _TC:
     self.w('unsigned it = 0;')
     self.open('for (size_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++it)')
     self.w(f'const unsigned db = it % {self.ND}u;')
-    self.w(f'if (!tfb_tc::mbar_wait(&bars[{self.BAR["dfull"]}u + db], (it / {self.ND}u) & 1u, {lim}ull)) '
+    self.w(f'if (!tfb_tc::{self.wfn}(&bars[{self.BAR["dfull"]}u + db], (it / {self.ND}u) & 1u, {lim}ull)) '
            f'{{ ok = false; atomicMax(&tfb_err_{b}, 20u); break; }}')
     self.w('tfb_tc::fence_after();')
     self.w(f'const unsigned dm = e_addr + {self.d_base}u + db * {self.dcols}u;')
@@ -1397,7 +1461,7 @@ class _TC:
     self.w(f'tfb_tc::mbar_arrive(&bars[{self.BAR["dfree"]}u + db]);')
     self.w(f'const size_t pel = tile * {te}u + ele;')
     staged = ('off_ost' in self.sm and out.addressing.name == 'STRIDED' and not s.accumulate
-              and out.element_volume() == M * s.N and M % 4 == 0)
+              and out.element_volume() == M * s.N and M % 4 == 0 and int(self.plan.params.get('ostage', 1)))
     if staged:
       # the warp's 32 rows are 32 consecutive output columns of the tile: stage them in
       # shared memory and write them with one bulk copy (unmasked, 16-byte aligned output)
@@ -1407,7 +1471,24 @@ class _TC:
       self.w(f'float* const ost = reinterpret_cast<float*>(tfb_smem_raw + {self.sm["off_ost"]});')
       orows = self.sm['ost_rows']
       self.w(f'const size_t nrows = (numElements - tile * {te}u) < {te}u ? (numElements - tile * {te}u) * {s.N}u : {te * s.N}u;')
-      for h in range(32 // orows):
+      if self.opad:
+        # padded rows (pitch M + 4 floats): each lane stages its row and issues its own bulk
+        # copy; a lane waits for its own earlier copies, and the warp syncs before another
+        # half of the lanes reuses the rows
+        OP = self.sm['ost_pitch']
+        for h in range(32 // orows):
+          self.w(f'{"if (it > 0) " if h == 0 else ""}tfb_tc::bulk_wait_read();  // this lane\'s earlier copies have read the buffer')
+          self.w('__syncwarp();')
+          self.open(f'if (ecol && (lane / {orows}u) == {h}u)')
+          self.w(f'float* const orow = ost + (equad * {orows}u + (lane - {h * orows}u)) * {OP}u;')
+          self.w('#pragma unroll')
+          self.w(f'for (int i = 0; i < {M // 4}; ++i) reinterpret_cast<float4*>(orow)[i] = '
+                 'make_float4(acc[4 * i], acc[4 * i + 1], acc[4 * i + 2], acc[4 * i + 3]);')
+          self.w('tfb_tc::fence_proxy_async();')
+          self.w('const size_t r = equad * 32u + lane;')
+          self.w(f'if (r < nrows) tfb_tc::bulk_store(obase + r * {M}u, orow, {M * 4}u);')
+          self.close()
+      for h in range(32 // orows if not self.opad else 0):
         # rows [r0, r0 + orows) of the warp go through its buffer of orows rows
         self.w(f'if (lane == 0 && (it > 0{" || true" if h else ""})) tfb_tc::bulk_wait_read();  // the buffer\'s previous copy has read it')
         self.w('__syncwarp();')
@@ -1449,7 +1530,7 @@ class _TC:
     self.close()
     self.close()
     if staged:
-      self.w('if (lane == 0) tfb_tc::bulk_wait();  // the last bulk stores have landed')
+      self.w(f'{"" if self.opad else "if (lane == 0) "}tfb_tc::bulk_wait();  // the last bulk stores have landed')
     self.close()
 
   # ------------------------------------------------------------------ producer
@@ -1552,7 +1633,7 @@ class _TC:
       kp = self.lay['kpad'][ti]
       acols = self.lay['a_cols'][ti]
       slot_col = slot_base[ti]
-      self.w(f'if (it > 0 && !tfb_tc::mbar_wait(&bars[{nterms + ti}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, {30 + ti}u); }}')
+      self.w(f'if (it > 0 && !tfb_tc::{self.wfn}(&bars[{nterms + ti}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, {30 + ti}u); }}')
       self.w('tfb_tc::fence_after();')
       self.open(f'if (c0 < {kp}u)')
       self.w(f'tfb_tc::st_x8(lane_addr + {slot_col}u + c0, hv{reg});')
@@ -1576,7 +1657,7 @@ class _TC:
     kp = self.lay['kpad'][ti]
     acols = self.lay['a_cols'][ti]
     nterms = len(self.s.terms)
-    self.w(f'if (it > 0 && !tfb_tc::mbar_wait(&bars[{nterms + ti}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, {30 + ti}u); }}')
+    self.w(f'if (it > 0 && !tfb_tc::{self.wfn}(&bars[{nterms + ti}], (it - 1u) & 1u, {lim}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, {30 + ti}u); }}')
     self.w('tfb_tc::fence_after();')
     if self.pipe == 2 and prec == 'tf32x3' and vec and t.K % 4 == 0 and LC == 16 and -(-kp // LC) <= H:
       # one body for all groups: group g takes columns [16 g, 16 g + 16) of the slot (keeps

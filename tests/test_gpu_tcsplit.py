@@ -122,7 +122,9 @@ PIPE3_OPTIONS = [{'form': 'u', 'qreg': 1}, {'form': 'u', 'slots': 2}, {'form': '
                  {'form': 'u', 'urows': 2}, {'form': 'u', 'urows': 2, 'fuse': 1}, {'form': 'u', 'qreg': 1, 'fuse': 1},
                  {'form': 'u', 'urows': 2, 'loader': 2}, {'form': 'u', 'urows': 2, 'fuse': 1, 'loader': 2},
                  {'form': 'u', 'urows': 1, 'fuse': 0, 'loader': 0},
-                 {'form': 'u', 'fuse': 0}, {'form': 'u', 'loader': 3}]
+                 {'form': 'u', 'fuse': 0}, {'form': 'u', 'loader': 3}, {'form': 'u', 'sleep': 0},
+                 {'form': 'u', 'sleep': 0, 'loader': 2}, {'form': 'u', 'ostage': 0},
+                 {'form': 'u', 'opad': 1}, {'form': 'u', 'uwarp': 1}, {'form': 'u', 'opad': 1, 'uwarp': 1}]
 
 
 @pytest.mark.parametrize('variant', PIPE3_OPTIONS, ids=lambda v: ','.join(f'{k}={x}' for k, x in v.items() if k != 'form'))
