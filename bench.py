@@ -141,6 +141,18 @@ def make_inputs(gen, n, device, seed, dist='uniform', dtype=None):
   return bufs
 
 
+def kernel_error(k, gen):
+  """Error word of a generated tensor-core kernel (a bounded wait that ran out), read and
+  cleared; 0 for kernels without one."""
+  import ctypes
+  f = getattr(ctypes.CDLL(k.so_path), f'tfb_kernel_error_{gen.get_base_name()}', None)
+  if f is None:
+    return 0
+  f.argtypes = [ctypes.c_void_p]
+  f.restype = ctypes.c_int
+  return int(f(None))
+
+
 def check_accuracy(descrs, gen, bufs, n_check):
   """Relative-L2 and max-abs error of the first n_check elements vs the FP64 oracle."""
   import numpy as np
@@ -588,8 +600,8 @@ def impl_ours(args, rank, world, dist):
              'tf32x3_spin': {'precision': 'tf32x3', 'variant': {'form': 'u', 'sleep': 0}},
              'tf32x3_ds': {'precision': 'tf32x3', 'variant': {'form': 'u', 'ostage': 0}},
              'tf32x3_op': {'precision': 'tf32x3', 'variant': {'form': 'u', 'opad': 1}},
-             'tf32x3_uw': {'precision': 'tf32x3', 'variant': {'form': 'u', 'uwarp': 1}},
-             'tf32x3_opuw': {'precision': 'tf32x3', 'variant': {'form': 'u', 'opad': 1, 'uwarp': 1}},
+             'tf32x3_nuw': {'precision': 'tf32x3', 'variant': {'form': 'u', 'uwarp': 0}},
+             'tf32x3_dl': {'precision': 'tf32x3', 'variant': {'form': 'u', 'direct': 1}},
 
              'plain_rs2': {'variant': {'strategy': 'colprog', 'threads': 256, 'rsplit': 2, 'min_blocks': 2}},
              'tf32x3_form_b': {'precision': 'tf32x3', 'variant': {'form': 'b'}},
@@ -623,9 +635,14 @@ def impl_ours(args, rank, world, dist):
     acc = check_accuracy(descrs, gen, bufs, min(n, 2048))
     steps = args.steps if primary is None else max(3, args.steps // 2)
     total, per = time_launches(fn, stream, steps, max(3, args.warmup), dist if primary is None else None)
+    err = kernel_error(k, gen)
     results[name] = {'kernel': gen.get_base_name(), 'plan': gen.get_plan().key(), 'ms_total': total,
                      'launch_ms': per, 'accuracy': acc, 'gen': gen, 'k': k, 'kw': kw}
-    ok = name == 'plain' or acc['rel_l2'] <= 1e-6
+    if err:
+      # a bounded wait ran out: the timing is not the kernel's, the variant is not reported
+      log(f'variant {name}: kernel error word {err} (a bounded wait ran out); not used')
+      results[name]['kernel_error'] = err
+    ok = (name == 'plain' or acc['rel_l2'] <= 1e-6) and not err
     if primary is None:
       # the choice changes the collective sequence (timed barriers): every rank must agree
       ok = ranks.all_ranks(ok, dist)
@@ -640,6 +657,8 @@ def impl_ours(args, rank, world, dist):
   # the timed region of record: K steps of the primary variant, clocks sampled meanwhile
   with Clocks(index=torch.cuda.current_device()) as clocks:
     total, per = time_launches(lambda: k(**kw), stream, args.steps, args.warmup, dist)
+  if kernel_error(k, gen):
+    raise RuntimeError(f'{primary}: a bounded wait ran out during the timed region')
   ms = ranks.max_over_ranks(total / args.steps, dist)
   value = ranks.aggregate_rate(world, n, ms)
 
@@ -707,7 +726,8 @@ def impl_ours(args, rank, world, dist):
   for name, r in results.items():
     extra_out.setdefault('variants', {})[name] = {
       'elements_per_s': n / (sum(r['launch_ms']) / len(r['launch_ms']) / 1e3), 'plan': r['plan'],
-      'rel_l2': r['accuracy']['rel_l2'], 'max_abs': r['accuracy']['max_abs']}
+      'rel_l2': r['accuracy']['rel_l2'], 'max_abs': r['accuracy']['max_abs'],
+      **({'kernel_error': r['kernel_error']} if 'kernel_error' in r else {})}
   # the link bound of the end-to-end step (contiguous copies of the same byte counts)
   link = link_bound(h2d, d2h)
   link['frac'] = link['duplex_ms'] / e_ms

@@ -195,6 +195,58 @@ def smem_plan_v3(shape, precision, qreg=False, fuse=False, rbuf2=False, opad=Fal
   return out
 
 
+def direct_ok(shape):
+  """The direct-lane producers need one per-element B operand shared by every term, an R
+  factor (batched, sparse or dense) in every term, all with the same K and P."""
+  t0 = shape.terms[0]
+  if t0.B is None or t0.B.kind != 'batched':
+    return False
+  for t in shape.terms:
+    if t.B is not t0.B or t.R is None or t.R.kind != 'batched' or t.K != t0.K or t.P != t0.P:
+      return False
+  return True
+
+
+def smem_plan_direct(shape, precision):
+  """Shared memory of the direct-lane producers: the B operand's hi / lo tiles (whole
+  N_mma-row tiles, back to back, for the fused MMA), two stages of the tile's per-element B
+  blocks, two dense pair buffers of the R factors (value (m, j) of term t for flat column
+  c = e * N + j at pair (t * P + m) * 128 + c, both halves the value, zeros outside the
+  pattern written once) and the output staging buffer."""
+  lay = layout(shape, precision)
+  te = lay['te']
+  tc = te * shape.N
+  t0 = shape.terms[0]
+  B = t0.B
+  bvals = _pad(B.element_volume(), 4)
+  stage = _pad(te * bvals * 4, 128)
+  r_ops = []
+  for t in shape.terms:
+    if all(t.R is not o for o in r_ops):
+      r_ops.append(t.R)
+  rows_b = lay['n_mma']
+  b_bytes = sum(2 * rows_b * kp * lay['es'] for kp in lay['kpad'])
+  off_stage = _pad(b_bytes, 128)
+  sd_bytes = _pad(len(shape.terms) * t0.P * 128 * 8, 128)
+  off_sd = off_stage + 2 * stage
+  off = off_sd + 2 * sd_bytes
+  out = dict(off_stage=off_stage, stage=stage, stage_off={B.name: 0}, b_ops=[B], r_ops=r_ops,
+             sdelta=stage // 4, off_sd=off_sd, sd_bytes=sd_bytes, sd_delta=sd_bytes // 8, rows_b=rows_b,
+             b_bytes=b_bytes, te=te, tc=tc, ost_rows=0, pitch=0, off_u=off, ubuf_bytes=0, bvals=bvals)
+  if shape.M % 4 == 0:
+    out['ost_pitch'] = shape.M
+    for rows in (32, 16):
+      ost = _pad(4 * rows * shape.M * 4, 128)
+      if off + ost + 256 <= _plan.SMEM_LIMIT:
+        out['off_ost'] = off
+        off += ost
+        out['ost_rows'] = rows
+        break
+  out['off_bar'] = off
+  out['total'] = off + 256
+  return out
+
+
 def pipe3_ok(shape, precision, chunk=16):
   """The warp-specialised pipeline (pipe 3) needs TF32 splits, a U pass for every term
   (K a multiple of 4, lane phases of at most 4 x 16 columns) and tensor memory for two A
@@ -266,8 +318,13 @@ def plan(chain, shape, precision, variant):
   loader_default = 3 if rbuf2_fits else 2
   rbuf2 = rbuf2_fits and int(variant.get('loader', loader_default)) == 3
   opad = pipe == 3 and bool(int(variant.get('opad', 0)))
-  sm = ((lambda sh, pr: smem_plan_v3(sh, pr, bool(int(variant.get('qreg', 0))), bool(fuse), rbuf2, opad))
-        if pipe == 3 else smem_plan_v2)(shape, precision) if pipe in (2, 3) else None
+  direct = pipe == 3 and bool(int(variant.get('direct', 0))) and direct_ok(shape) and not int(variant.get('qreg', 0))
+  if direct:
+    fuse, rbuf2, opad = 1, False, False
+    sm = smem_plan_direct(shape, precision)
+  else:
+    sm = ((lambda sh, pr: smem_plan_v3(sh, pr, bool(int(variant.get('qreg', 0))), bool(fuse), rbuf2, opad))
+          if pipe == 3 else smem_plan_v2)(shape, precision) if pipe in (2, 3) else None
   if sm is None or sm['total'] > _plan.SMEM_LIMIT:
     pipe = 1
     sm = smem_plan(shape, precision)
@@ -298,6 +355,12 @@ def plan(chain, shape, precision, variant):
     params['loader'] = int(variant.get('loader', loader_default))
     if params['loader'] == 3 and not rbuf2:
       params['loader'] = 2
+    if direct:
+      # direct-lane producers: each producer thread computes its own TMEM lane's columns of
+      # U_t from the B block (packed FMAs over the dense R pairs) and stores them to tensor
+      # memory; loader mode 4 double-buffers the B stage and scatters the R factors
+      params['direct'] = 1
+      params['loader'] = 4
     # option: the per-element B operand goes straight from global memory into registers one
     # tile ahead (two rows per producer), so the stage only holds the R blocks
     b_ops = {id(t.B) for t in shape.terms}
@@ -310,7 +373,8 @@ def plan(chain, shape, precision, variant):
     # hi*hi and hi*lo as one MMA of twice the width (B's hi and lo tiles back to back, the
     # main and correction accumulators side by side)
     params['fuse'] = 1
-  if int(variant.get('urows', 2 if pipe == 3 else 1)) == 2 and pipe in (2, 3) and all(t.K % 2 == 0 for t in shape.terms):
+  if (int(variant.get('urows', 2 if pipe == 3 else 1)) == 2 and pipe in (2, 3) and not direct
+      and all(t.K % 2 == 0 for t in shape.terms)):
     params['urows'] = 2
   if pipe == 3 and int(variant.get('sleep', 1)):
     # waiting threads sleep in try_wait (global-timer bound) instead of spinning, leaving
@@ -319,10 +383,12 @@ def plan(chain, shape, precision, variant):
     params['sleep'] = 1
   if opad:
     # option: output staging rows padded by 16 bytes (no bank conflicts on the staging
-    # stores), each row written by its own bulk copy
+    # stores), each row written by its own bulk copy (measured slower: 6.44e8 el/s against
+    # 6.51e8 with one bulk copy per 16 rows)
     params['opad'] = 1
-  if pipe == 3 and int(variant.get('uwarp', 0)):
-    # option: U pass work items aligned to warps (no warp straddles two elements)
+  if pipe == 3 and int(variant.get('uwarp', 1)) and not direct:
+    # U pass work items aligned to warps, so no warp straddles two elements (order-6 chain,
+    # 500,000 elements: 6.59e8 el/s against 6.51e8 with items spread over all threads)
     params['uwarp'] = 1
   if pipe == 3 and not int(variant.get('ostage', 1)):
     # option: the epilogue warps store their columns straight from registers (no staging)
@@ -498,7 +564,9 @@ class _TC:
     self.fuse = self.pipe == 3 and int(plan_.params.get('fuse', 0)) == 1
     self.rbuf2 = self.pipe == 3 and int(plan_.params.get('loader', 0)) == 3 and not self.qreg
     self.opad = self.pipe == 3 and bool(int(plan_.params.get('opad', 0)))
-    self.sm = (smem_plan_v3(shape, self.prec, self.qreg, self.fuse, self.rbuf2, self.opad) if self.pipe == 3 else
+    self.direct = self.pipe == 3 and bool(int(plan_.params.get('direct', 0)))
+    self.sm = (smem_plan_direct(shape, self.prec) if self.direct else
+               smem_plan_v3(shape, self.prec, self.qreg, self.fuse, self.rbuf2, self.opad) if self.pipe == 3 else
                smem_plan_v2(shape, self.prec) if self.pipe == 2 else smem_plan(shape, self.prec))
     self.LC = plan_.params['chunk']
     self.ahead = bool(plan_.params.get('ahead', 0))
@@ -590,6 +658,8 @@ class _TC:
       self.w(f'// {st.descr}')
     for ti, tbl in enumerate(gathers):
       self.w(f'__device__ const short bgather{ti}_{b}[{len(tbl)}] = {{{", ".join(str(x) for x in tbl)}}};')
+    if self.direct:
+      self._sd_table_decl()
     self.w(f'__device__ unsigned tfb_err_{b} = 0u;')
     self.w(f'extern "C" int tfb_kernel_error_{b}(void* stream) {{')
     self.w('  unsigned v = 0, z = 0;')
@@ -617,7 +687,7 @@ class _TC:
     # loader warp: 1 fetches all inputs of the next tile, 2 only the bulk copy of the B
     # blocks (the producers keep issuing the small R copies)
     self.loader_mode = int(self.plan.params.get('loader', 0)) if p3 else 0
-    self.loader = self.loader_mode in (1, 2, 3)
+    self.loader = self.loader_mode in (1, 2, 3, 4)
     nthreads = 32 * (4 * H + 1 + (4 if p3 else 0) + (1 if self.loader else 0))
     BAR_FULL, BAR_FREE, BAR_DFULL, BAR_DFREE = 0, nterms, 2 * nterms, 2 * nterms + 1
     if p3:
@@ -634,19 +704,27 @@ class _TC:
       self.BAR = dict(full=BAR_FULL, free=BAR_FREE, dfull=BAR_DFULL, dfree=BAR_DFREE,
                       stage=2 * self.NS + 2 * self.ND, sfree=2 * self.NS + 2 * self.ND + 1,
                       rstage=2 * self.NS + 2 * self.ND + 2)
+      if self.direct:
+        # two stage buffers, each with one barrier (bulk copy of B + the R scatter) and one
+        # release barrier (the producers have read it)
+        self.BAR['sfree'] = 2 * self.NS + 2 * self.ND + 2
 
     self.w(f'__global__ void __launch_bounds__({nthreads}, 1) {kname}({", ".join(self.params(globals_))}) {{')
     self.ind += 1
     self.w('extern __shared__ __align__(1024) unsigned char tfb_smem_raw[];')
     self.w(f'uint64_t* const bars = reinterpret_cast<uint64_t*>(tfb_smem_raw + {sm["off_bar"]});')
-    nbars = (2 * self.NS + 2 * self.ND + 2 + (2 if self.rbuf2 else 0)) if p3 else 2 * nterms + (3 if self.pipe == 2 else 2)
+    nbars = ((2 * self.NS + 2 * self.ND + (4 if self.direct else 2 + (2 if self.rbuf2 else 0))) if p3
+             else 2 * nterms + (3 if self.pipe == 2 else 2))
     BAR_STAGE = self.BAR['stage'] if p3 else 2 * nterms + 2
     self.w(f'unsigned* const tmem_slot = reinterpret_cast<unsigned*>(bars + {nbars});')
     probe = int(self.plan.params.get('wait_probe', 0))
     if probe:
       self.w(f'uint64_t* const probe_bar = bars + {nbars + 1};  // never arrived on')
       assert (nbars + 2) * 8 <= 256
-    if self.pipe in (2, 3):
+    if self.direct:
+      self.w(f'float* const stage = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_stage"]});')
+      self.w(f'float2* const sdp = reinterpret_cast<float2*>(tfb_smem_raw + {sm["off_sd"]});')
+    elif self.pipe in (2, 3):
       self.w(f'float* const stage = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_stage"]});')
       for ti in range(nterms):
         self.w(f'float* const ubuf{ti} = reinterpret_cast<float*>(tfb_smem_raw + {sm["off_u"] + ti * sm["ubuf_bytes"]});')
@@ -678,6 +756,11 @@ class _TC:
         self.w(f'*reinterpret_cast<__nv_bfloat16*>(tfb_smem_raw + {hi_off} + boff) = h;')
         self.w(f'*reinterpret_cast<__nv_bfloat16*>(tfb_smem_raw + {lo_off} + boff) = l;')
       self.close()
+    if self.direct:
+      # the dense R pair buffers: zeros outside the patterns, written once
+      self.open(f'for (int q = threadIdx.x; q < {2 * sm["sd_bytes"] // 16}; q += blockDim.x)')
+      self.w('reinterpret_cast<float4*>(sdp)[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);')
+      self.close()
     self.open('if (threadIdx.x == 0)')
     if p3:
       for i in range(self.NS):
@@ -686,7 +769,7 @@ class _TC:
       for i in range(self.ND):
         self.w(f'tfb_tc::mbar_init(&bars[{BAR_DFULL + i}], 1u);')
         self.w(f'tfb_tc::mbar_init(&bars[{BAR_DFREE + i}], 128u);')
-      if self.loader:
+      if self.loader and not self.direct:
         self.w(f'tfb_tc::mbar_init(&bars[{self.BAR["sfree"]}], 1u);')
     else:
       for ti in range(nterms):
@@ -694,7 +777,14 @@ class _TC:
         self.w(f'tfb_tc::mbar_init(&bars[{BAR_FREE + ti}], 1u);')
       self.w(f'tfb_tc::mbar_init(&bars[{BAR_DFULL}], 1u);')
       self.w(f'tfb_tc::mbar_init(&bars[{BAR_DFREE}], {NP}u);')
-    if self.pipe in (2, 3):
+    if self.direct:
+      # per stage buffer: the B copy's arrival (bulk expect_tx, or lane 0 after the cp.async
+      # fallback) + the 32 loader lanes' cp.async arrivals of the R scatter; its release
+      # barrier counts the producer warps
+      for i in range(2):
+        self.w(f'tfb_tc::mbar_init(&bars[{BAR_STAGE + i}], 33u);')
+        self.w(f'tfb_tc::mbar_init(&bars[{self.BAR["sfree"] + i}], {NP // 32}u);')
+    elif self.pipe in (2, 3):
       # one arrival per copying thread (cp.async completion) + the bulk-copy issuer's expect_tx
       stage_count = {1: 32 + 1, 3: 1}.get(self.loader_mode, NP + 1)
       self.w(f'tfb_tc::mbar_init(&bars[{BAR_STAGE}], {stage_count}u);')
@@ -754,7 +844,11 @@ class _TC:
       self.close()
       self.close()
     # ---- producers
-    if p3:
+    if p3 and self.direct:
+      self._producers_direct(s, te, tcols, NP, lim, BAR_STAGE)
+      self._epilogue_warps_v3(s, te, tcols, lim, n_mma)
+      self._loader_direct(stage_off, lim, BAR_STAGE)
+    elif p3:
       self._producers_v3(s, te, tcols, NP, stage_off, lim, BAR_STAGE)
       self._epilogue_warps_v3(s, te, tcols, lim, n_mma)
       if self.loader:
@@ -1339,10 +1433,12 @@ class _TC:
       self.close()
     self.close()
 
-  def _bulk_b_only(self, tile_expr, stage_off, BAR_STAGE):
+  def _bulk_b_only(self, tile_expr, stage_off, BAR_STAGE, dst='stage', bar=None):
     """Loader mode 2: the B blocks of a tile, one bulk copy by lane 0 with its expect_tx
     arrival; when a block is misaligned the 32 lanes copy it with cp.async, wait for their
-    copies and lane 0 arrives (one arrival either way)."""
+    copies and lane 0 arrives (one arrival either way). `dst` and `bar` select another stage
+    buffer and its barrier (loader mode 4)."""
+    bar = bar if bar is not None else f'bars[{BAR_STAGE}]'
     sm = self.sm
     te = sm['te']
     b_ops = sm['b_ops']
@@ -1359,19 +1455,19 @@ class _TC:
     per_elem = sum(op.element_volume() * 4 for op in b_ops)
     self.open('if (bulk_in)')
     self.open('if (lane == 0)')
-    self.w(f'tfb_tc::mbar_arrive_expect_tx(&bars[{BAR_STAGE}], bnv * {per_elem}u);')
+    self.w(f'tfb_tc::mbar_arrive_expect_tx(&{bar}, bnv * {per_elem}u);')
     for op in b_ops:
-      self.w(f'tfb_tc::bulk_load(stage + {stage_off[op.name]}, {op.name} + be0 * {op.element_volume()}u + '
-             f'{op.name}_extraOffset, bnv * {op.element_volume() * 4}u, &bars[{BAR_STAGE}]);')
+      self.w(f'tfb_tc::bulk_load({dst} + {stage_off[op.name]}, {op.name} + be0 * {op.element_volume()}u + '
+             f'{op.name}_extraOffset, bnv * {op.element_volume() * 4}u, &{bar});')
     self.close()
     self.close()
     self.open('else')
     for op in b_ops:
-      self._cp_async_copy(op, op.element_volume(), stage_off[op.name], tile_expr, 'stage', 32)
+      self._cp_async_copy(op, op.element_volume(), stage_off[op.name], tile_expr, dst, 32)
     self.w('tfb_tc::cp_async_commit();  // wait_group only waits for committed copies')
     self.w('tfb_tc::cp_async_wait_all();')
     self.w('__syncwarp();')
-    self.w(f'if (lane == 0) tfb_tc::mbar_arrive(&bars[{BAR_STAGE}]);')
+    self.w(f'if (lane == 0) tfb_tc::mbar_arrive(&{bar});')
     self.close()
     self.close()
 
@@ -1422,6 +1518,221 @@ class _TC:
     self.w(f'if (pending && !tfb_tc::{self.wfn}(&bars[{BAR_STAGE}], (it - 1u) & 1u, {lim}ull)) atomicMax(&tfb_err_{b}, 41u);')
     self.w('tfb_tc::cp_async_wait_all();')
     self.w('if (lane == 0) tfb_tc::bulk_wait();')
+    self.close()
+
+  def _sd_slots(self):
+    """(term, storage position) pairs of the R factors in scatter order, with each one's pair
+    index (t * P + m) * 128 + j in the dense pair buffer (the element adds e * N)."""
+    s = self.s
+    P, N = s.terms[0].P, s.N
+    slots = []
+    for ti, t in enumerate(s.terms):
+      R = t.R
+      if R.sparse:
+        look = R.sparse_lookup()
+        inv = {pos: mj for mj, pos in look.items()}
+        nv = R.storage_size()
+      else:
+        inv = {j * P + m: (m, j) for m in range(P) for j in range(N)}
+        nv = P * N
+      for pos in range(nv):
+        m, j = inv[pos]
+        slots.append((ti, pos, (ti * P + m) * 128 + j))
+    return slots
+
+  def _sd_table_decl(self):
+    """File-scope table of the loader lanes' R scatter slots: one packed word per slot, pair
+    index + 1 (0: no slot) in bits 0-15, term in bits 16-23, storage position in 24-31."""
+    slots = self._sd_slots()
+    nsl = len(slots)
+    kq = (nsl + 31) // 32
+    assert all(sl[2] + 1 < (1 << 16) and sl[1] < 256 for sl in slots)
+    words = [((d + 1) | (ti << 16) | (pos << 24)) for ti, pos, d in slots] + [0] * (32 * kq - nsl)
+    self.sd_kq = kq
+    self.w(f'__device__ const unsigned sdslot_{self.base}[{32 * kq}] = {{{", ".join(f"{w_}u" for w_ in words)}}};')
+
+  def _producers_direct(self, s, te, tcols, NP, lim, BAR_STAGE):
+    """Direct-lane producers: producer (quadrant, group) owns TMEM lane row = flat column
+    c = e * N + j of the tile and the K columns [16 grp, 16 grp + 16). Per tile: wait for the
+    stage buffer, compute U_t[l, c] = sum_m B_e[l, m] R_t[m, j] for its K columns and every
+    term (m ascending, packed FMAs over two rows with the dense R pair (R, R); zeros outside
+    R's pattern), release the stage, then per term split into TF32 hi / lo and store them to
+    that term's A slot."""
+    b, H = self.base, self.H
+    sm = self.sm
+    nterms = len(s.terms)
+    t0 = s.terms[0]
+    K, P, N = t0.K, t0.P, s.N
+    kp = self.lay['kpad'][0]
+    half = self.scols // 2
+    NS, BR = self.NS, self.BAR
+    bvals = sm['bvals']
+    self.open(f'else if (warp < {4 * H})')
+    self.w('const unsigned quad = warp & 3u, grp = warp >> 2;')
+    self.w('const unsigned row = quad * 32u + lane;')
+    self.w('const unsigned lane_addr = tmem + ((quad * 32u) << 16);')
+    self.w(f'const bool lane_col = row < {tcols}u;')
+    self.w(f'const unsigned le = row / {N}u;')
+    self.w(f'const unsigned lec = le < {te}u ? le : {te - 1}u;  // in-bounds stage reads for the padding lanes')
+    self.w('const unsigned c0 = grp * 16u;')
+    self.w('const float2 neg1 = make_float2(-1.0f, -1.0f);')
+    self.w('unsigned it = 0;')
+    self.open('for (size_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++it)')
+    self.w('// every producer takes the same branches around the barrier: a timeout anywhere stops')
+    self.w('// all producers at the next tile boundary (a barrier-wide OR), never mid-tile')
+    self.w(f'if (tfb_tc::any_sync(1, {NP}, !ok)) break;')
+    self.w('const unsigned sb = it & 1u;')
+    self.w(f'if (!tfb_tc::{self.wfn}(&bars[{BAR_STAGE}u + sb], (it >> 1) & 1u, {lim}ull)) '
+           f'{{ ok = false; atomicMax(&tfb_err_{b}, 40u); }}')
+    self.w(f'const float* const qs = stage + (sb ? {sm["sdelta"]}u : 0u) + lec * {bvals}u + c0;')
+    self.w(f'const float2* const sd = sdp + (sb ? {sm["sd_delta"]}u : 0u) + row;')
+    self.w(f'float2 acc[{nterms}][8];')
+    self.w(f'for (int t = 0; t < {nterms}; ++t) for (int p = 0; p < 8; ++p) acc[t][p] = make_float2(0.0f, 0.0f);')
+    # full groups (16 columns) and the last, partial group
+    ncols_list = sorted({min(16, K - 16 * g) for g in range(H) if K - 16 * g > 0}, reverse=True)
+    for idx, ncols in enumerate(ncols_list):
+      if len(ncols_list) == 1:
+        self.open(f'if (c0 < {K}u)')
+      elif idx == 0:
+        self.open(f'if (c0 + {ncols}u <= {K}u)')
+      else:
+        self.open(f'else if (c0 < {K}u)')
+      nv4 = ncols // 4
+      for m in range(P):
+        self.open('')
+        for ti in range(nterms):
+          self.w(f'const float2 s{ti} = sd[{(ti * P + m) * 128}];')
+        # the row in halves of 8 columns: fewer live registers, the same loads
+        for h0 in range(0, nv4, 2):
+          self.open('')
+          for v in range(h0, min(nv4, h0 + 2)):
+            self.w(f'const float4 x{v} = *reinterpret_cast<const float4*>(qs + {m * K + 4 * v});')
+          for ti in range(nterms):
+            for v in range(h0, min(nv4, h0 + 2)):
+              self.w(f'acc[{ti}][{2 * v}] = __ffma2_rn(make_float2(x{v}.x, x{v}.y), s{ti}, acc[{ti}][{2 * v}]);')
+              self.w(f'acc[{ti}][{2 * v + 1}] = __ffma2_rn(make_float2(x{v}.z, x{v}.w), s{ti}, acc[{ti}][{2 * v + 1}]);')
+          self.close()
+        self.close()
+      self.close()
+    self.w('__syncwarp();')
+    self.w(f'if (lane == 0) tfb_tc::mbar_arrive(&bars[{BR["sfree"]}u + sb]);  // this warp has read the stage buffer')
+    self.w(f'const size_t el = tile * {te}u + le;')
+    self.w('const bool active = lane_col && el < numElements && (flags == nullptr || flags[el] != 0u);')
+    for ti in range(nterms):
+      self.open('')
+      self.w(f'const unsigned chunk = it * {nterms}u + {ti}u, sl = chunk % {NS}u;')
+      self.w(f'if (chunk >= {NS}u && !tfb_tc::{self.wfn}(&bars[{BR["free"]}u + sl], ((chunk - {NS}u) / {NS}u) & 1u, {lim}ull)) '
+             f'{{ ok = false; atomicMax(&tfb_err_{b}, {30 + ti}u); }}')
+      self.w('tfb_tc::fence_after();')
+      self.w(f'const unsigned slot = lane_addr + sl * {self.scols}u;')
+      self.open(f'if (c0 < {kp}u)')
+      self.w('unsigned hv[16], lv[16];')
+      self.w('#pragma unroll')
+      self.open('for (int p = 0; p < 8; ++p)')
+      self.w(f'const float2 u = active ? acc[{ti}][p] : make_float2(0.0f, 0.0f);')
+      self.w('hv[2 * p] = tfb_tc::tf32_rna(u.x);')
+      self.w('hv[2 * p + 1] = tfb_tc::tf32_rna(u.y);')
+      self.w('const float2 lo = __ffma2_rn(make_float2(__uint_as_float(hv[2 * p]), __uint_as_float(hv[2 * p + 1])), neg1, u);')
+      self.w('lv[2 * p] = __float_as_uint(lo.x);')
+      self.w('lv[2 * p + 1] = __float_as_uint(lo.y);')
+      self.close()
+      self.w('tfb_tc::st_x8(slot + c0, hv);')
+      self.w(f'tfb_tc::st_x8(slot + {half}u + c0, lv);')
+      self.open(f'if (c0 + 8u < {kp}u)')
+      self.w('tfb_tc::st_x8(slot + c0 + 8u, hv + 8);')
+      self.w(f'tfb_tc::st_x8(slot + {half}u + c0 + 8u, lv + 8);')
+      self.close()
+      self.close()
+      self.w('tfb_tc::st_wait();')
+      self.w('tfb_tc::fence_before();')
+      self.w(f'tfb_tc::mbar_arrive(&bars[{BR["full"]}u + sl]);')
+      self.close()
+    self.close()
+    self.close()
+
+  def _loader_direct(self, stage_off, lim, BAR_STAGE):
+    """Loader mode 4 (direct-lane producers): tiles it and it + 1 in flight in two stage
+    buffers. Once the producers have released buffer it & 1 (its own release barrier, so a
+    release two tiles ahead cannot alias), the warp fills it with tile it + 2: the bulk copy
+    of the B blocks, and the R values scattered as (R, R) pairs into the dense pair buffer
+    by 4-byte cp.async copies (lane q takes the (term, position) slots q, q + 32, ... of
+    every element), each lane's copies counted on the buffer's barrier."""
+    b = self.base
+    sm = self.sm
+    te, N = sm['te'], self.s.N
+    kq = self.sd_kq
+    self.open('else')
+    self.w('const unsigned ptid = lane;')
+    for k in range(kq):
+      self.w(f'const unsigned sw{k} = sdslot_{b}[{32 * k}u + lane];')
+      self.w(f'const int sdst{k} = (int)(sw{k} & 0xFFFFu) - 1;')
+      self.w(f'const unsigned sterm{k} = (sw{k} >> 16) & 0xFFu, spos{k} = sw{k} >> 24;')
+    r_of_term = [t.R for t in self.s.terms]
+    ptr_based = [R.addressing.name == 'PTR_BASED' for R in r_of_term]
+    # per slot, once per CTA: the R operand's base (strided: the first element's value at
+    # the slot's position; pointer arrays: the pointer table, the position added per element)
+    for k in range(kq):
+      if any(ptr_based):
+        self.w(f'const float* const* sptab{k} = nullptr; unsigned soff{k} = 0u;')
+      self.w(f'const float* sbase{k} = nullptr; unsigned svol{k} = 0u;')
+      for ti, R in enumerate(r_of_term):
+        self.open(f'{"if" if ti == 0 else "else if"} (sterm{k} == {ti}u)')
+        if ptr_based[ti]:
+          self.w(f'sptab{k} = {R.name}; soff{k} = {R.name}_extraOffset + spos{k};')
+        else:
+          self.w(f'sbase{k} = {R.name} + {R.name}_extraOffset + spos{k}; svol{k} = {R.element_volume()}u;')
+        self.close()
+
+    def src_expr(k, e):
+      if not any(ptr_based):
+        return f'sbase{k} + ({e}) * svol{k}'
+      if all(ptr_based):
+        return f'sptab{k}[{e}] + soff{k}'
+      return f'(sptab{k} != nullptr ? sptab{k}[{e}] + soff{k} : sbase{k} + ({e}) * svol{k})'
+
+    def fill(tile_expr, buf_expr):
+      bar = f'bars[{BAR_STAGE}u + (({buf_expr}) ? 1u : 0u)]'
+      self._bulk_b_only(tile_expr, stage_off, BAR_STAGE, dst=f'(stage + (({buf_expr}) ? {sm["sdelta"]}u : 0u))', bar=bar)
+      self.open('')
+      self.w(f'float* const sdf = reinterpret_cast<float*>(sdp + (({buf_expr}) ? {sm["sd_delta"]}u : 0u));')
+      self.w(f'const size_t fe0 = ({tile_expr}) * {te}u;')
+      self.w(f'const unsigned fnv = (unsigned)((numElements - fe0) < {te}u ? (numElements - fe0) : {te}u);')
+      self.w('#pragma unroll 2')
+      self.open('for (unsigned ei = 0; ei < fnv; ++ei)')
+      for k in range(kq):
+        self.open(f'if (sdst{k} >= 0)')
+        self.w(f'const float* const src = {src_expr(k, "fe0 + ei")};')
+        self.w(f'float* const dst = sdf + 2u * ((unsigned)sdst{k} + ei * {N}u);')
+        self.w('tfb_tc::cp_async4(dst, src);')
+        self.w('tfb_tc::cp_async4(dst + 1, src);')
+        self.close()
+      self.close()
+      self.w(f'tfb_tc::cp_async_mbar_arrive(&{bar});')
+      self.w('tfb_tc::cp_async_commit();')
+      self.close()
+
+    self.w('unsigned nis0 = 0, nis1 = 0;  // fills issued into each buffer')
+    self.open('if ((size_t)blockIdx.x < numTiles)')
+    fill('(size_t)blockIdx.x', '0u')
+    self.w('++nis0;')
+    self.close()
+    self.open('if ((size_t)blockIdx.x + gridDim.x < numTiles)')
+    fill('(size_t)blockIdx.x + gridDim.x', '1u')
+    self.w('++nis1;')
+    self.close()
+    self.w('unsigned it = 0;')
+    self.open('for (size_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++it)')
+    self.w('const size_t nt = tile + 2u * (size_t)gridDim.x;')
+    self.w('if (nt >= numTiles) continue;')
+    self.w(f'if (!tfb_tc::{self.wfn}(&bars[{self.BAR["sfree"]}u + (it & 1u)], (it >> 1) & 1u, {lim}ull)) '
+           f'{{ ok = false; atomicMax(&tfb_err_{b}, 42u); break; }}')
+    fill('nt', 'it & 1u')
+    self.w('if (it & 1u) ++nis1; else ++nis0;')
+    self.close()
+    self.w('// fills still in flight must land before the CTA exits (consumed, or not after an abort)')
+    self.w(f'if (nis0 && !tfb_tc::{self.wfn}(&bars[{BAR_STAGE}], (nis0 - 1u) & 1u, {lim}ull)) atomicMax(&tfb_err_{b}, 41u);')
+    self.w(f'if (nis1 && !tfb_tc::{self.wfn}(&bars[{BAR_STAGE + 1}], (nis1 - 1u) & 1u, {lim}ull)) atomicMax(&tfb_err_{b}, 41u);')
+    self.w('tfb_tc::cp_async_wait_all();')
     self.close()
 
   def _epilogue_warps_v3(self, s, te, tcols, lim, n_mma):

@@ -124,7 +124,8 @@ PIPE3_OPTIONS = [{'form': 'u', 'qreg': 1}, {'form': 'u', 'slots': 2}, {'form': '
                  {'form': 'u', 'urows': 1, 'fuse': 0, 'loader': 0},
                  {'form': 'u', 'fuse': 0}, {'form': 'u', 'loader': 3}, {'form': 'u', 'sleep': 0},
                  {'form': 'u', 'sleep': 0, 'loader': 2}, {'form': 'u', 'ostage': 0},
-                 {'form': 'u', 'opad': 1}, {'form': 'u', 'uwarp': 1}, {'form': 'u', 'opad': 1, 'uwarp': 1}]
+                 {'form': 'u', 'opad': 1}, {'form': 'u', 'uwarp': 0},
+                 {'form': 'u', 'direct': 1}]
 
 
 @pytest.mark.parametrize('variant', PIPE3_OPTIONS, ids=lambda v: ','.join(f'{k}={x}' for k, x in v.items() if k != 'form'))
@@ -148,13 +149,18 @@ def test_warp_specialised_pipeline_options_flags_loguniform(variant):
   assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-6
 
 
+@pytest.mark.parametrize('direct', [0, 1])
 @pytest.mark.parametrize('n', [1, 333, 2001])
-def test_warp_specialised_pipeline_pointer_arrays(n):
+def test_warp_specialised_pipeline_pointer_arrays(n, direct):
   """Q, S and out through device arrays of element pointers: the B blocks take the copy
-  fallback (no contiguous tile), the output the per-lane stores."""
-  g = __import__('tensorforge_b200.kernels', fromlist=['make']).make('chain_o6_ptr', 'float', precision='tf32x3')
+  fallback (no contiguous tile), the output the per-lane stores; with the direct-lane
+  producers the loader reads the S values through the pointer tables."""
+  variant = {'form': 'u', 'direct': direct}
+  g = __import__('tensorforge_b200.kernels', fromlist=['make']).make('chain_o6_ptr', 'float', precision='tf32x3',
+                                                                     variant=variant)
   assert g.get_plan().params['pipe'] == 3
-  got, ref, _, _ = _run('chain_o6_ptr', 'tf32x3', n)
+  assert int(g.get_plan().params.get('direct', 0)) == direct
+  got, ref, _, _ = _run('chain_o6_ptr', 'tf32x3', n, variant=variant)
   assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-6
 
 
