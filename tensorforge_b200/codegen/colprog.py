@@ -326,9 +326,15 @@ class _ColProg:
 
     The group's ABI symbols arrive through a tfb_group_args record (pointers, extra offsets,
     element count, flags); A is read from shared memory (staged when the group changes).
+    With the plan's prefetch stage the group also gets `group<g>_prefetch` (cp.async of a
+    tile's batched inputs into the stage), and its tile function takes the next work item's
+    tile when that item belongs to the same group (~0 otherwise) and fetches it during its
+    last K stage.
     """
     assert self.asrc == 'smem'
     s, T, BT = self.s, self.T, self.BT
+    if self.prefetch:
+      self.next_tile = 'next_tile'
     self._layout()
     self._header()
     decl = []
@@ -347,12 +353,25 @@ class _ColProg:
       self.w(f'for (int q = threadIdx.x; q < {t.A.storage_size()}; q += {BT}) sA[{self.a_base[ti]} + q] = {t.A.name}[q];')
     self.ind -= 1
     self.w('}')
-    self.w(f'__device__ __forceinline__ void group{gid}_tile(const tfb_group_args& ga, size_t tile, {T}* ubuf, const {T}* sA) {{')
+    if self.prefetch:
+      self.w(f'__device__ __forceinline__ void group{gid}_prefetch(const tfb_group_args& ga, size_t tile, {T}* ubuf) {{')
+      self.ind += 1
+      for d in decl:
+        self.w(d)
+      self.w('const size_t numElements = (size_t)ga.num_elements;')
+      self._prefetch('tile')
+      self.ind -= 1
+      self.w('}')
+    nxt = ', size_t next_tile' if self.prefetch else ''
+    self.w(f'__device__ __forceinline__ void group{gid}_tile(const tfb_group_args& ga, size_t tile, {T}* ubuf, const {T}* sA{nxt}) {{')
     self.ind += 1
     for d in decl:
       self.w(d)
     self.w('const size_t numElements = (size_t)ga.num_elements;')
     self.w('const unsigned* const flags = ga.flags;')
+    if self.prefetch:
+      self.w('tfb_cp::wait_all();  // this tile\'s stage has landed')
+      self.w('__syncthreads();')
     self._tile_body()
     self.ind -= 1
     self.w('}')
@@ -467,8 +486,13 @@ class _ColProg:
     self.w('__syncthreads();')
     if self.prefetch and ti == len(s.terms) - 1:
       self.w('// the stage is free: fetch the next tile while this K stage runs')
-      self.open('if (tile + gridDim.x < numTiles)')
-      self._prefetch('tile + gridDim.x')
+      if getattr(self, 'next_tile', None) is None:
+        self.open('if (tile + gridDim.x < numTiles)')
+        self._prefetch('tile + gridDim.x')
+      else:
+        # grouped launch: the next work item when it belongs to the same group
+        self.open(f'if ({self.next_tile} != ~(size_t)0)')
+        self._prefetch(self.next_tile)
       self.close()
       self.w('tfb_cp::commit();')
     # K stage: each A value is an FMA operand for every column the thread owns

@@ -114,7 +114,7 @@ def _bulk_eligible(op, vals):
   return op.addressing.name == 'STRIDED' and op.element_volume() == vals and (vals * 4) % 16 == 0
 
 
-def smem_plan_v2(shape, precision):
+def smem_plan_v2(shape, precision, l64=False):
   """Shared memory of the one-pass pipeline: single input stage (B blocks first, the tile's
   output staged over them, R blocks behind both) and one transposition buffer per term."""
   lay = layout(shape, precision)
@@ -136,7 +136,12 @@ def smem_plan_v2(shape, precision):
     off += te * _pad(op.storage_size() if op.sparse else op.element_volume(), 4)
   stage = _pad(off * 4, 128)
   kmax = max(t.K for t in shape.terms)
+  # transposition rows: 16-byte aligned for the lane phase's 128-bit loads, or (l64) a pitch
+  # of 2 mod 32 words so that 16 consecutive rows fall on distinct bank pairs for 64-bit loads
   pitch = _pad(kmax, 4) + 4
+  if l64:
+    # row r's 64-bit word w sits on bank pair (r * pitch / 2 + w) mod 16: pitch / 2 odd
+    pitch = _pad(kmax, 2) + (2 if (_pad(kmax, 2) // 2) % 2 == 0 else 0)
   ubuf = _pad(tc * pitch * 4, 128)
   off_stage = _pad(lay['b_bytes'], 128)
   off_u = off_stage + stage
@@ -146,14 +151,14 @@ def smem_plan_v2(shape, precision):
               pitch=pitch, ubuf_bytes=ubuf, off_bar=off_bar, total=total, te=te, tc=tc)
 
 
-def smem_plan_v3(shape, precision, qreg=False, fuse=False, rbuf2=False, opad=False):
+def smem_plan_v3(shape, precision, qreg=False, fuse=False, rbuf2=False, opad=False, l64=False):
   """Shared memory of the warp-specialised pipeline: the one-pass layout, an output staging
   buffer for the epilogue warps' bulk stores (32 rows per warp, or 16 rows at a time when
   only that fits) and the B operand. Without `fuse` B is stored for the real output rows
   only (rows M..N_mma-1 of the MMA's B tile then read the next block and land in
   accumulator columns the epilogue never reads); with `fuse` each term's hi and lo blocks
   are whole N_mma-row tiles, back to back, read by one MMA of width 2 N_mma."""
-  sm = smem_plan_v2(shape, precision)
+  sm = smem_plan_v2(shape, precision, l64)
   if qreg:
     # the stage holds the R blocks only (B is read into registers)
     off = 0
@@ -323,7 +328,8 @@ def plan(chain, shape, precision, variant):
     fuse, rbuf2, opad = 1, False, False
     sm = smem_plan_direct(shape, precision)
   else:
-    sm = ((lambda sh, pr: smem_plan_v3(sh, pr, bool(int(variant.get('qreg', 0))), bool(fuse), rbuf2, opad))
+    l64 = pipe == 3 and bool(int(variant.get('l64', 0)))
+    sm = ((lambda sh, pr: smem_plan_v3(sh, pr, bool(int(variant.get('qreg', 0))), bool(fuse), rbuf2, opad, l64))
           if pipe == 3 else smem_plan_v2)(shape, precision) if pipe in (2, 3) else None
   if sm is None or sm['total'] > _plan.SMEM_LIMIT:
     pipe = 1
@@ -386,6 +392,10 @@ def plan(chain, shape, precision, variant):
     # stores), each row written by its own bulk copy (measured slower: 6.44e8 el/s against
     # 6.51e8 with one bulk copy per 16 rows)
     params['opad'] = 1
+  if pipe == 3 and int(variant.get('l64', 0)) and not direct:
+    # option: the lane phase reads the transposition rows with 64-bit loads (rows of a pitch
+    # that keeps 16 consecutive rows on distinct bank pairs)
+    params['l64'] = 1
   if pipe == 3 and int(variant.get('uwarp', 1)) and not direct:
     # U pass work items aligned to warps, so no warp straddles two elements (order-6 chain,
     # 500,000 elements: 6.59e8 el/s against 6.51e8 with items spread over all threads)
@@ -565,8 +575,9 @@ class _TC:
     self.rbuf2 = self.pipe == 3 and int(plan_.params.get('loader', 0)) == 3 and not self.qreg
     self.opad = self.pipe == 3 and bool(int(plan_.params.get('opad', 0)))
     self.direct = self.pipe == 3 and bool(int(plan_.params.get('direct', 0)))
+    self.l64 = self.pipe == 3 and bool(int(plan_.params.get('l64', 0))) and not self.direct
     self.sm = (smem_plan_direct(shape, self.prec) if self.direct else
-               smem_plan_v3(shape, self.prec, self.qreg, self.fuse, self.rbuf2, self.opad) if self.pipe == 3 else
+               smem_plan_v3(shape, self.prec, self.qreg, self.fuse, self.rbuf2, self.opad, self.l64) if self.pipe == 3 else
                smem_plan_v2(shape, self.prec) if self.pipe == 2 else smem_plan(shape, self.prec))
     self.LC = plan_.params['chunk']
     self.ahead = bool(plan_.params.get('ahead', 0))
@@ -1271,9 +1282,14 @@ class _TC:
     self.w('for (int i = 0; i < 16; ++i) u[i] = 0.0f;')
     self.open('if (active)')
     self.w(f'const float* p = {src} + c0;')
-    for v in range(4):
-      self.w(f'if (c0 + {4 * v}u < {t.K}u) {{ const float4 x = *reinterpret_cast<const float4*>(p + {4 * v}); '
-             f'u[{4*v}] = x.x; u[{4*v+1}] = x.y; u[{4*v+2}] = x.z; u[{4*v+3}] = x.w; }}')
+    if self.l64:
+      for v in range(8):
+        self.w(f'if (c0 + {2 * v}u < {t.K}u) {{ const float2 x = *reinterpret_cast<const float2*>(p + {2 * v}); '
+               f'u[{2*v}] = x.x; u[{2*v+1}] = x.y; }}')
+    else:
+      for v in range(4):
+        self.w(f'if (c0 + {4 * v}u < {t.K}u) {{ const float4 x = *reinterpret_cast<const float4*>(p + {4 * v}); '
+               f'u[{4*v}] = x.x; u[{4*v+1}] = x.y; u[{4*v+2}] = x.z; u[{4*v+3}] = x.w; }}')
     self.close()
     self.w('unsigned hv[16], lv[16];')
     self.w('#pragma unroll')

@@ -44,7 +44,7 @@ class _GroupArgs(ctypes.Structure):
 
 
 class GroupedKernel:
-  def __init__(self, generators, threads=256, name=None):
+  def __init__(self, generators, threads=256, name=None, prefetch=False):
     if not generators:
       raise GenerationError('a grouped launch needs at least one chain')
     self.gens = generators
@@ -65,7 +65,10 @@ class GroupedKernel:
           raise GenerationError('scalar operands are not supported in grouped launches')
       if len(g.abi_symbols()) > MAX_SYMBOLS:
         raise GenerationError(f'at most {MAX_SYMBOLS} operands per group')
-    key = ','.join(g.get_base_name() for g in generators) + f'|{threads}'
+    # prefetch: each group's tile fetches the next work item's inputs (same group) into a
+    # cp.async stage during its last K stage, as the standalone column programs do
+    self.prefetch = bool(prefetch)
+    key = ','.join(g.get_base_name() for g in generators) + f'|{threads}' + ('|pf' if self.prefetch else '')
     self.name = name or 'grouped_' + hashlib.md5(key.encode()).hexdigest()[:10]
     self._emit()
     self._lib = None
@@ -75,10 +78,11 @@ class GroupedKernel:
     self.te = []
     for gid, g in enumerate(self.gens):
       shape = match_left_chain(g.get_chain())
-      plan = Plan('colprog', {'threads': self.threads, 'chunk': 16, 'a_source': 'smem', 'prefetch': 0})
+      plan = Plan('colprog', {'threads': self.threads, 'chunk': 16, 'a_source': 'smem',
+                              'prefetch': 1 if self.prefetch else 0})
       em = _ColProg(g.get_chain(), shape, plan, g.get_context(), f'{self.name}_g{gid}')
       parts.append(em.emit_group_functions(g.abi_symbols(), gid))
-      work_vals = max(work_vals, em.work_vals)
+      work_vals = max(work_vals, em.work_vals + em.stage_vals)
       a_vals = max(a_vals, _pad(em.a_total, 4))
       self.te.append(em.TE)
     self.smem = (work_vals + a_vals) * self.fs
@@ -104,21 +108,34 @@ class GroupedKernel:
     k.append('    if ((int)wi.x != cur) {')
     k.append('      switch (wi.x) {')
     for gid in range(len(self.gens)):
-      k.append(f'        case {gid}u: group{gid}_stage_a(args[{gid}], sA); break;')
+      pf = f' group{gid}_prefetch(args[{gid}], (size_t)wi.y, ubuf);' if self.prefetch else ''
+      k.append(f'        case {gid}u: group{gid}_stage_a(args[{gid}], sA);{pf} break;')
     k.append('        default: break;')
     k.append('      }')
+    if self.prefetch:
+      k.append('      tfb_cp::commit();')
     k.append('      __syncthreads();')
     k.append('      cur = (int)wi.x;')
     k.append('    }')
+    nxt = ''
+    if self.prefetch:
+      # the claimed next item, known to every thread, decides the prefetch of this tile
+      k.append('    __syncthreads();')
+      k.append('    const unsigned nx = s_item[nb];')
+      k.append('    size_t next_tile = ~(size_t)0;')
+      k.append('    if (nx < num_items) { const uint2 wn = items[nx]; if (wn.x == wi.x) next_tile = (size_t)wn.y; }')
+      nxt = ', next_tile'
     k.append('    switch (wi.x) {')
     for gid in range(len(self.gens)):
-      k.append(f'      case {gid}u: group{gid}_tile(args[{gid}], (size_t)wi.y, ubuf, sA); break;')
+      k.append(f'      case {gid}u: group{gid}_tile(args[{gid}], (size_t)wi.y, ubuf, sA{nxt}); break;')
     k.append('      default: break;')
     k.append('    }')
     k.append('    __syncthreads();')
     k.append('    item = s_item[nb];')
     k.append('    nb ^= 1u;')
     k.append('  }')
+    if self.prefetch:
+      k.append('  tfb_cp::wait_all();')
     k.append('}')
     k.append('')
     k.append(f'extern "C" int tfb_grouped_launch_{self.name}(const void* args, const void* items, unsigned num_items, '
@@ -203,7 +220,12 @@ class GroupedKernel:
           '    }',
           '    switch (grp) {']
     for gid in range(G):
-      k.append(f'      case {gid}u: group{gid}_tile(prm.args[{gid}], (size_t)tile, ubuf, sA); break;')
+      if self.prefetch:
+        # no look-ahead here: the tile's inputs are fetched right before it
+        k.append(f'      case {gid}u: group{gid}_prefetch(prm.args[{gid}], (size_t)tile, ubuf); tfb_cp::commit(); '
+                 f'group{gid}_tile(prm.args[{gid}], (size_t)tile, ubuf, sA, ~(size_t)0); break;')
+      else:
+        k.append(f'      case {gid}u: group{gid}_tile(prm.args[{gid}], (size_t)tile, ubuf, sA); break;')
     k += ['      default: break;',
           '    }',
           '    __syncthreads();',

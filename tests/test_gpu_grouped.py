@@ -63,6 +63,20 @@ def test_grouped_matches_oracle():
   _check(descrs, per)
 
 
+@pytest.mark.parametrize('threads', [128, 256])
+def test_grouped_prefetch_matches_oracle(threads):
+  """Each tile fetches the next same-group work item's inputs during its last K stage."""
+  import torch
+  from tensorforge_b200.grouped import GroupedKernel
+  gens, descrs = _groups()
+  gk = GroupedKernel(gens, threads=threads, prefetch=True)
+  per = _setup(descrs, use_flags=True)
+  launch = gk.prepare([p[3] for p in per])
+  launch.launch()
+  torch.cuda.synchronize()
+  _check(descrs, per)
+
+
 def test_grouped_flags_and_graph_replay():
   import torch
   from tensorforge_b200.grouped import GroupedKernel
