@@ -44,7 +44,7 @@ class _GroupArgs(ctypes.Structure):
 
 
 class GroupedKernel:
-  def __init__(self, generators, threads=256, name=None, prefetch=False):
+  def __init__(self, generators, threads=256, name=None, prefetch=True):
     if not generators:
       raise GenerationError('a grouped launch needs at least one chain')
     self.gens = generators
@@ -66,7 +66,10 @@ class GroupedKernel:
       if len(g.abi_symbols()) > MAX_SYMBOLS:
         raise GenerationError(f'at most {MAX_SYMBOLS} operands per group')
     # prefetch: each group's tile fetches the next work item's inputs (same group) into a
-    # cp.async stage during its last K stage, as the standalone column programs do
+    # cp.async stage during its last K stage, as the standalone column programs do (config 3,
+    # 1.5M mixed-shape elements: 33.9 ms against 38.5 ms without; 128 threads per CTA
+    # measured 40.3 ms without and 59.5 ms with the stage, whose shared memory then leaves
+    # one CTA per SM)
     self.prefetch = bool(prefetch)
     key = ','.join(g.get_base_name() for g in generators) + f'|{threads}' + ('|pf' if self.prefetch else '')
     self.name = name or 'grouped_' + hashlib.md5(key.encode()).hexdigest()[:10]

@@ -63,13 +63,15 @@ def test_grouped_matches_oracle():
   _check(descrs, per)
 
 
-@pytest.mark.parametrize('threads', [128, 256])
-def test_grouped_prefetch_matches_oracle(threads):
-  """Each tile fetches the next same-group work item's inputs during its last K stage."""
+@pytest.mark.parametrize('threads,prefetch', [(128, True), (256, False)])
+def test_grouped_variants_match_oracle(threads, prefetch):
+  """128 threads per CTA with the prefetch stage (each tile fetches the next same-group work
+  item's inputs during its last K stage; the default at 256 threads), and 256 threads
+  without it."""
   import torch
   from tensorforge_b200.grouped import GroupedKernel
   gens, descrs = _groups()
-  gk = GroupedKernel(gens, threads=threads, prefetch=True)
+  gk = GroupedKernel(gens, threads=threads, prefetch=prefetch)
   per = _setup(descrs, use_flags=True)
   launch = gk.prepare([p[3] for p in per])
   launch.launch()
