@@ -407,6 +407,10 @@ def plan(chain, shape, precision, variant):
     # failure-detection check: the kernel first waits, with this many polls, on an mbarrier
     # that nothing arrives on, records error 30 and returns before issuing any copy or MMA
     params['wait_probe'] = int(variant['wait_probe'])
+  if int(variant.get('wait_probe_ns', 0)) > 0:
+    # the same check for the sleeping wait: it gives up after this many nanoseconds of the
+    # global timer
+    params['wait_probe_ns'] = int(variant['wait_probe_ns'])
   return Plan('tcsplit', params, smem, 32 * (4 * H_GROUPS + 1),
               note=f'M={shape.M} N={shape.N} terms={len(shape.terms)} tmem={lay["tmem_used"]} smem={sm["total"]}')
 
@@ -728,7 +732,8 @@ class _TC:
              else 2 * nterms + (3 if self.pipe == 2 else 2))
     BAR_STAGE = self.BAR['stage'] if p3 else 2 * nterms + 2
     self.w(f'unsigned* const tmem_slot = reinterpret_cast<unsigned*>(bars + {nbars});')
-    probe = int(self.plan.params.get('wait_probe', 0))
+    probe_ns = int(self.plan.params.get('wait_probe_ns', 0))
+    probe = int(self.plan.params.get('wait_probe', 0)) or probe_ns
     if probe:
       self.w(f'uint64_t* const probe_bar = bars + {nbars + 1};  // never arrived on')
       assert (nbars + 2) * 8 <= 256
@@ -817,7 +822,10 @@ class _TC:
     self.w('bool ok = true;')
     if probe:
       # nothing has been issued yet: on timeout every thread goes straight to the teardown
-      self.w(f'if (threadIdx.x == 0 && !tfb_tc::mbar_wait(probe_bar, 0u, {probe}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 30u); }}')
+      if probe_ns:
+        self.w(f'if (threadIdx.x == 0 && !tfb_tc::mbar_wait_s(probe_bar, 0u, {probe_ns}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 30u); }}')
+      else:
+        self.w(f'if (threadIdx.x == 0 && !tfb_tc::mbar_wait(probe_bar, 0u, {probe}ull)) {{ ok = false; atomicMax(&tfb_err_{b}, 30u); }}')
       self.w('ok = __syncthreads_and(ok ? 1 : 0) != 0;')
       self.open('if (ok)')
     # ---- MMA issuer

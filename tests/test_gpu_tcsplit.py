@@ -257,18 +257,23 @@ def test_form_u_split_ahead(n):
     assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-6
 
 
-def test_bounded_wait_runs_out_and_context_stays_usable():
-  """Failure detection without a fault: a kernel built with a 4,096-poll wait on an
-  mbarrier that nothing arrives on (plan option `wait_probe`, before any copy or MMA is
+@pytest.mark.parametrize('probe', [{'wait_probe': 4096}, {'wait_probe_ns': 50000000}],
+                         ids=['polls', 'global_timer'])
+def test_bounded_wait_runs_out_and_context_stays_usable(probe):
+  """Failure detection without a fault: a kernel built with a bounded wait on an mbarrier
+  that nothing arrives on (plan option `wait_probe`: 4,096 polls of the spinning wait, or
+  `wait_probe_ns`: 50 ms of the global timer in the sleeping wait; before any copy or MMA is
   issued) gives up, records error 30 in its error word and returns; the launch itself
   succeeds, the outputs are untouched, reading the error word clears it, and the regular
   kernel then runs in the same context and matches the oracle."""
+  import time
   import torch
   from tensorforge_b200.kernels import make
   from tensorforge_b200.runtime import compile_generator
   n = 333
-  g = make('chain_o6', 'float', precision='tf32x3', variant={'wait_probe': 4096})
-  assert g.get_plan().params.get('wait_probe') == 4096
+  g = make('chain_o6', 'float', precision='tf32x3', variant=probe)
+  key, val = next(iter(probe.items()))
+  assert g.get_plan().params.get(key) == val
   k = compile_generator(g)
   descrs = cases.build('chain_o6', cases.ns_from_module('tensorforge_b200'))
   lay, mem = harness.make_memory(descrs, n, seed=5)
@@ -280,8 +285,13 @@ def test_bounded_wait_runs_out_and_context_stays_usable():
       kw[f'{l.name}_extraOffset'] = l.extra_offset
   out = [l for l in lay if l.kind == 'strided' and l.tensor.direction.name != 'SOURCE'][0]
   before = dev[out.name].clone()
+  torch.cuda.synchronize()
+  t0 = time.time()
   k(**kw)
   torch.cuda.synchronize()
+  if key == 'wait_probe_ns':
+    # the sleeping wait gave up after its time limit, not earlier
+    assert time.time() - t0 >= val * 1e-9
   errf = getattr(ctypes.CDLL(k.so_path), f'tfb_kernel_error_{g.get_base_name()}')
   errf.argtypes = [ctypes.c_void_p]
   assert errf(None) == 30
