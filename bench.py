@@ -603,6 +603,7 @@ def impl_ours(args, rank, world, dist):
              'tf32x3_nuw': {'precision': 'tf32x3', 'variant': {'form': 'u', 'uwarp': 0}},
              'tf32x3_dl': {'precision': 'tf32x3', 'variant': {'form': 'u', 'direct': 1}},
              'tf32x3_l64': {'precision': 'tf32x3', 'variant': {'form': 'u', 'l64': 1}},
+             'tf32x3_oswz': {'precision': 'tf32x3', 'variant': {'form': 'u', 'oswz': 1}},
 
              'plain_rs2': {'variant': {'strategy': 'colprog', 'threads': 256, 'rsplit': 2, 'min_blocks': 2}},
              'tf32x3_form_b': {'precision': 'tf32x3', 'variant': {'form': 'b'}},

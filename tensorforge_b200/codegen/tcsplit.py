@@ -400,6 +400,9 @@ def plan(chain, shape, precision, variant):
     # U pass work items aligned to warps, so no warp straddles two elements (order-6 chain,
     # 500,000 elements: 6.59e8 el/s against 6.51e8 with items spread over all threads)
     params['uwarp'] = 1
+  if pipe == 3 and int(variant.get('oswz', 0)):
+    # option: the output staging stores of rows 4r..4r+3 (r odd) swap each chunk pair
+    params['oswz'] = 1
   if pipe == 3 and not int(variant.get('ostage', 1)):
     # option: the epilogue warps store their columns straight from registers (no staging)
     params['ostage'] = 0
@@ -580,6 +583,7 @@ class _TC:
     self.opad = self.pipe == 3 and bool(int(plan_.params.get('opad', 0)))
     self.direct = self.pipe == 3 and bool(int(plan_.params.get('direct', 0)))
     self.l64 = self.pipe == 3 and bool(int(plan_.params.get('l64', 0))) and not self.direct
+    self.oswz = self.pipe == 3 and bool(int(plan_.params.get('oswz', 0)))
     self.sm = (smem_plan_direct(shape, self.prec) if self.direct else
                smem_plan_v3(shape, self.prec, self.qreg, self.fuse, self.rbuf2, self.opad, self.l64) if self.pipe == 3 else
                smem_plan_v2(shape, self.prec) if self.pipe == 2 else smem_plan(shape, self.prec))
@@ -1806,6 +1810,17 @@ class _TC:
       self.w(f'float* const ost = reinterpret_cast<float*>(tfb_smem_raw + {self.sm["off_ost"]});')
       orows = self.sm['ost_rows']
       self.w(f'const size_t nrows = (numElements - tile * {te}u) < {te}u ? (numElements - tile * {te}u) * {s.N}u : {te * s.N}u;')
+      swz = self.oswz and not self.opad and (M // 4) % 2 == 0
+      if swz:
+        # rows 4r..4r+3 with r odd write each pair of 16-byte chunks in swapped order: the 8
+        # rows of a store phase then fall on 8 distinct bank groups (a row is 14 chunks)
+        self.w('const unsigned sw = (lane >> 2) & 1u;')
+        self.w('#pragma unroll')
+        self.open(f'for (int i = 0; i < {M // 4}; i += 2)')
+        self.w('#pragma unroll')
+        self.w('for (int q = 0; q < 4; ++q) { const float t = acc[4 * i + q]; '
+               'acc[4 * i + q] = sw ? acc[4 * i + 4 + q] : t; acc[4 * i + 4 + q] = sw ? t : acc[4 * i + 4 + q]; }')
+        self.close()
       if self.opad:
         # padded rows (pitch M + 4 floats): each lane stages its row and issues its own bulk
         # copy; a lane waits for its own earlier copies, and the warp syncs before another
@@ -1830,9 +1845,14 @@ class _TC:
         self.w('// rows past the tile\'s columns have no place in the buffer')
         self.open(f'if (ecol && (lane / {orows}u) == {h}u)')
         self.w(f'float* const orow = ost + (equad * {orows}u + (lane - {h * orows}u)) * {M}u;')
-        self.w('#pragma unroll')
-        self.w(f'for (int i = 0; i < {M // 4}; ++i) reinterpret_cast<float4*>(orow)[i] = '
-               'make_float4(acc[4 * i], acc[4 * i + 1], acc[4 * i + 2], acc[4 * i + 3]);')
+        if swz:
+          self.w('#pragma unroll')
+          self.w(f'for (int i = 0; i < {M // 4}; ++i) reinterpret_cast<float4*>(orow)[i ^ sw] = '
+                 'make_float4(acc[4 * i], acc[4 * i + 1], acc[4 * i + 2], acc[4 * i + 3]);')
+        else:
+          self.w('#pragma unroll')
+          self.w(f'for (int i = 0; i < {M // 4}; ++i) reinterpret_cast<float4*>(orow)[i] = '
+                 'make_float4(acc[4 * i], acc[4 * i + 1], acc[4 * i + 2], acc[4 * i + 3]);')
         self.close()
         self.w('tfb_tc::fence_proxy_async();')
         self.w('__syncwarp();')
