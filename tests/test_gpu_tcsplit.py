@@ -300,3 +300,44 @@ def test_bounded_wait_runs_out_and_context_stays_usable(probe):
   assert torch.equal(dev[out.name], before)
   got, ref, _, _ = _run('chain_o6', 'tf32x3', n, seed=5)
   assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-6
+
+
+@pytest.mark.parametrize('precision,variant', [('tf32x3', None), ('tf32x3', {'form': 'u', 'direct': 1}),
+                                               ('tf32x3', {'pipe': 2}), (None, None)],
+                         ids=['ws_pipeline', 'direct_lanes', 'one_pass', 'plain_fp32'])
+def test_empty_batch_and_all_masked_elements(precision, variant):
+  """Edge cases of the launcher contract: numElements = 0 launches nothing and returns 0;
+  with every flag 0 the kernel runs over all tiles and writes no output value. In both the
+  outputs keep their previous contents bit for bit and the error word stays 0."""
+  import torch
+  from tensorforge_b200.kernels import make
+  from tensorforge_b200.runtime import compile_generator
+  kw_make = {}
+  if precision:
+    kw_make['precision'] = precision
+  if variant:
+    kw_make['variant'] = variant
+  g = make('chain_o6', 'float', **kw_make)
+  k = compile_generator(g)
+  n = 333
+  descrs = cases.build('chain_o6', cases.ns_from_module('tensorforge_b200'))
+  lay, mem = harness.make_memory(descrs, n, seed=9)
+  dev, kw = {}, {'numElements': n}
+  for l in lay:
+    dev[l.name] = torch.tensor(mem.buffers[l.name], dtype=torch.float32, device='cuda')
+    kw[l.name] = dev[l.name]
+    if l.kind == 'strided':
+      kw[f'{l.name}_extraOffset'] = l.extra_offset
+  out = [l for l in lay if l.kind == 'strided' and l.tensor.direction.name != 'SOURCE'][0]
+  before = dev[out.name].clone()
+  k(**dict(kw, numElements=0))
+  torch.cuda.synchronize()
+  assert torch.equal(dev[out.name], before)
+  kw['flags'] = torch.zeros(n, dtype=torch.int32, device='cuda')
+  k(**kw)
+  torch.cuda.synchronize()
+  assert torch.equal(dev[out.name], before)
+  errf = getattr(ctypes.CDLL(k.so_path), f'tfb_kernel_error_{g.get_base_name()}', None)
+  if errf is not None:
+    errf.argtypes = [ctypes.c_void_p]
+    assert errf(None) == 0
