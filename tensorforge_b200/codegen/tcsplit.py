@@ -400,6 +400,11 @@ def plan(chain, shape, precision, variant):
     # U pass work items aligned to warps, so no warp straddles two elements (order-6 chain,
     # 500,000 elements: 6.59e8 el/s against 6.51e8 with items spread over all threads)
     params['uwarp'] = 1
+  if pipe == 3 and int(variant.get('estg', 0)):
+    # option: the epilogue reads the accumulators in 16x256b fragments and stores whole
+    # 32-byte sectors straight to global memory (no output staging; measured slower: 6.51e8
+    # against 6.59e8 el/s with the staging buffer and bulk copies)
+    params['estg'] = 1
   if pipe == 3 and int(variant.get('oswz', 0)):
     # option: the output staging stores of rows 4r..4r+3 (r odd) swap each chunk pair
     # (measured no gain: 6.57e8 against 6.58e8 el/s)
@@ -512,6 +517,12 @@ __device__ __forceinline__ void ld_x8(unsigned taddr, unsigned* v) {
                : "r"(taddr) : "memory");
 }
 __device__ __forceinline__ void ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// 16 lanes x 256 bits from [taddr]: thread t receives words 2 (t % 4), 2 (t % 4) + 1 of lanes
+// t / 4 (v[0], v[1]) and t / 4 + 8 (v[2], v[3])
+__device__ __forceinline__ void ld16x256(unsigned taddr, unsigned* v) {
+  asm volatile("tcgen05.ld.sync.aligned.16x256b.x1.b32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]) : "r"(taddr) : "memory");
+}
 // round to nearest TF32 (10 stored mantissa bits); the result is exactly representable
 __device__ __forceinline__ unsigned tf32_rna(float x) {
   unsigned r;
@@ -585,6 +596,7 @@ class _TC:
     self.direct = self.pipe == 3 and bool(int(plan_.params.get('direct', 0)))
     self.l64 = self.pipe == 3 and bool(int(plan_.params.get('l64', 0))) and not self.direct
     self.oswz = self.pipe == 3 and bool(int(plan_.params.get('oswz', 0)))
+    self.estg = self.pipe == 3 and bool(int(plan_.params.get('estg', 0)))
     self.sm = (smem_plan_direct(shape, self.prec) if self.direct else
                smem_plan_v3(shape, self.prec, self.qreg, self.fuse, self.rbuf2, self.opad, self.l64) if self.pipe == 3 else
                smem_plan_v2(shape, self.prec) if self.pipe == 2 else smem_plan(shape, self.prec))
@@ -1785,6 +1797,42 @@ class _TC:
            f'{{ ok = false; atomicMax(&tfb_err_{b}, 20u); break; }}')
     self.w('tfb_tc::fence_after();')
     self.w(f'const unsigned dm = e_addr + {self.d_base}u + db * {self.dcols}u;')
+    estg = (self.estg and out.addressing.name == 'STRIDED' and not s.accumulate
+            and out.element_volume() == M * s.N and M % 8 == 0)
+    if estg:
+      # 16x256b reads: each group of 4 threads holds 8 consecutive values of one output
+      # column, so every warp store writes whole 32-byte sectors (no staging buffer)
+      vol = out.element_volume()
+      self.w(f'float* const obase = {out.name} + tile * {te * vol}u + {out.name}_extraOffset;')
+      self.open('if (flags == nullptr && (reinterpret_cast<uintptr_t>(obase) & 7u) == 0u)')
+      self.w(f'float ev[{2 * nld * 4}];')
+      for h in range(2):
+        for k0 in range(0, nld, 2):
+          ks = list(range(k0, min(nld, k0 + 2)))
+          self.open('')
+          self.w(f'unsigned dv[{4 * len(ks)}], dc[{4 * len(ks)}];')
+          for i, k in enumerate(ks):
+            self.w(f'tfb_tc::ld16x256(dm + {(16 * h) << 16}u + {8 * k}u, dv + {4 * i});')
+            self.w(f'tfb_tc::ld16x256(dm + {(16 * h) << 16}u + {n_mma + 8 * k}u, dc + {4 * i});')
+          self.w('tfb_tc::ld_wait();')
+          self.w('#pragma unroll')
+          self.w(f'for (int i = 0; i < {4 * len(ks)}; ++i) ev[{(h * nld + k0) * 4} + i] = __uint_as_float(dv[i]) + __uint_as_float(dc[i]);')
+          self.close()
+      self.w('tfb_tc::fence_before();')
+      self.w(f'tfb_tc::mbar_arrive(&bars[{self.BAR["dfree"]}u + db]);')
+      self.w(f'const size_t nrows = (numElements - tile * {te}u) < {te}u ? (numElements - tile * {te}u) * {s.N}u : {te * s.N}u;')
+      self.w('const unsigned er = equad * 32u + (lane >> 2), ew = 2u * (lane & 3u);')
+      for h in range(2):
+        for half in range(2):
+          c = f'er + {16 * h + 8 * half}u'
+          self.open(f'if ({c} < nrows)')
+          self.w(f'float* const ocol = obase + (size_t)({c}) * {M}u + ew;')
+          for k in range(nld):
+            base = (h * nld + k) * 4 + 2 * half
+            self.w(f'*reinterpret_cast<float2*>(ocol + {8 * k}) = make_float2(ev[{base}], ev[{base + 1}]);')
+          self.close()
+      self.close()
+      self.open('else')
     self.w(f'float acc[{nld * 8}];')
     for k0 in range(0, nld, 2):
       ks = list(range(k0, min(nld, k0 + 2)))
@@ -1801,7 +1849,8 @@ class _TC:
     self.w(f'tfb_tc::mbar_arrive(&bars[{self.BAR["dfree"]}u + db]);')
     self.w(f'const size_t pel = tile * {te}u + ele;')
     staged = ('off_ost' in self.sm and out.addressing.name == 'STRIDED' and not s.accumulate
-              and out.element_volume() == M * s.N and M % 4 == 0 and int(self.plan.params.get('ostage', 1)))
+              and out.element_volume() == M * s.N and M % 4 == 0 and int(self.plan.params.get('ostage', 1))
+              and not estg)
     if staged:
       # the warp's 32 rows are 32 consecutive output columns of the tile: stage them in
       # shared memory and write them with one bulk copy (unmasked, 16-byte aligned output)
@@ -1884,6 +1933,8 @@ class _TC:
       self.w('#pragma unroll')
       self.w(f'for (int i = 0; i < {M}; ++i) col[i] = acc[i];')
     self.close()
+    if estg:
+      self.close()   # the else branch of the sector-store path
     self.close()
     if staged:
       self.w(f'{"" if self.opad else "if (lane == 0) "}tfb_tc::bulk_wait();  // the last bulk stores have landed')
