@@ -598,6 +598,8 @@ def impl_ours(args, rank, world, dist):
              'tf32x3_nf': {'precision': 'tf32x3', 'variant': {'form': 'u', 'fuse': 0}},
              'tf32x3_l3': {'precision': 'tf32x3', 'variant': {'form': 'u', 'loader': 3}},
              'tf32x3_spin': {'precision': 'tf32x3', 'variant': {'form': 'u', 'sleep': 0}},
+             'tf32x3_sl1': {'precision': 'tf32x3', 'variant': {'form': 'u', 'sleep': 1}},
+             'tf32x3_sl2': {'precision': 'tf32x3', 'variant': {'form': 'u', 'sleep': 2}},
              'tf32x3_ds': {'precision': 'tf32x3', 'variant': {'form': 'u', 'ostage': 0}},
              'tf32x3_op': {'precision': 'tf32x3', 'variant': {'form': 'u', 'opad': 1}},
              'tf32x3_nuw': {'precision': 'tf32x3', 'variant': {'form': 'u', 'uwarp': 0}},

@@ -382,11 +382,13 @@ def plan(chain, shape, precision, variant):
   if (int(variant.get('urows', 2 if pipe == 3 else 1)) == 2 and pipe in (2, 3) and not direct
       and all(t.K % 2 == 0 for t in shape.terms)):
     params['urows'] = 2
-  if pipe == 3 and int(variant.get('sleep', 1)):
+  if pipe == 3 and int(variant.get('sleep', 3)):
     # waiting threads sleep in try_wait (global-timer bound) instead of spinning, leaving
-    # the issue slots to the producers (order-6 chain, 500,000 elements: 6.51e8 el/s
-    # against 6.45e8 with spinning waits)
-    params['sleep'] = 1
+    # the issue slots to the producers (order-6 chain, 500,000 elements: 6.51e8 el/s with
+    # every role sleeping against 6.45e8 spinning); the default 3 keeps the MMA thread
+    # spinning, so it issues as soon as a lane phase arrives (6.61e8 against 6.58e8 with
+    # every role sleeping and 6.46e8 with the producers spinning too, option 2)
+    params['sleep'] = int(variant.get('sleep', 3))
   if opad:
     # option: output staging rows padded by 16 bytes (no bank conflicts on the staging
     # stores), each row written by its own bulk copy (measured slower: 6.44e8 el/s against
@@ -713,9 +715,17 @@ class _TC:
     d_main, d_corr = col, col + n_mma
     p3 = self.pipe == 3
     # waits that sleep in try_wait (bounded by the global timer) or spin (bounded by polls)
-    sleep = p3 and bool(int(self.plan.params.get('sleep', 0)))
+    sleep = int(self.plan.params.get('sleep', 0)) if p3 else 0
     self.wfn = 'mbar_wait_s' if sleep else 'mbar_wait'
     lim = self.WAIT_NS if sleep else self.WAIT_LIMIT
+    # which roles sleep: 1 all; 2 the epilogue and loader warps (the producers and the MMA
+    # thread spin); 3 all but the MMA thread
+    spin_roles = {2: ('mma', 'producers'), 3: ('mma',)}.get(sleep, ())
+
+    def role(name):
+      spin = name in spin_roles or not sleep
+      self.wfn = 'mbar_wait' if spin else 'mbar_wait_s'
+      return self.WAIT_LIMIT if spin else self.WAIT_NS
     # loader warp: 1 fetches all inputs of the next tile, 2 only the bulk copy of the B
     # blocks (the producers keep issuing the small R copies)
     self.loader_mode = int(self.plan.params.get('loader', 0)) if p3 else 0
@@ -847,7 +857,7 @@ class _TC:
       self.open('if (ok)')
     # ---- MMA issuer
     if p3:
-      self._mma_v3(s, lay, b_off, ke, es, idesc, lim, n_mma)
+      self._mma_v3(s, lay, b_off, ke, es, idesc, role('mma'), n_mma)
     else:
       self.open(f'if (warp == {4 * H})')
       self.open('if (lane == 0)')
@@ -885,10 +895,11 @@ class _TC:
       self._epilogue_warps_v3(s, te, tcols, lim, n_mma)
       self._loader_direct(stage_off, lim, BAR_STAGE)
     elif p3:
-      self._producers_v3(s, te, tcols, NP, stage_off, lim, BAR_STAGE)
-      self._epilogue_warps_v3(s, te, tcols, lim, n_mma)
+      self._producers_v3(s, te, tcols, NP, stage_off, role('producers'), BAR_STAGE)
+      self._epilogue_warps_v3(s, te, tcols, role('epilogue'), n_mma)
       if self.loader:
-        self._loader_v3(stage_off, lim, BAR_STAGE)
+        self._loader_v3(stage_off, role('loader'), BAR_STAGE)
+      role('rest')
     elif self.pipe == 2:
       self._producers_v2(s, te, tcols, NP, stage_off, slot_base, lim, BAR_DFULL, BAR_STAGE, d_main, d_corr)
     else:
