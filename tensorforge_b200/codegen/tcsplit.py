@@ -402,6 +402,14 @@ def plan(chain, shape, precision, variant):
     # U pass work items aligned to warps, so no warp straddles two elements (order-6 chain,
     # 500,000 elements: 6.59e8 el/s against 6.51e8 with items spread over all threads)
     params['uwarp'] = 1
+  if pipe == 3 and int(variant.get('lpk', 1)):
+    # the lane phase forms lo = u - hi with packed FMAs (exact) and stores 16 columns per
+    # tensor-memory store (order-6 chain, 500,000 elements: 6.76e8 el/s against 6.63e8 with
+    # scalar subtractions and 8-column stores)
+    params['lpk'] = 1
+  if pipe == 3 and int(variant.get('epk', 0)):
+    # option: the epilogue sums the main and correction accumulators with packed adds
+    params['epk'] = 1
   if pipe == 3 and int(variant.get('estg', 0)):
     # option: the epilogue reads the accumulators in 16x256b fragments and stores whole
     # 32-byte sectors straight to global memory (no output staging; measured slower: 6.51e8
@@ -511,6 +519,11 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
 __device__ __forceinline__ void st_x8(unsigned taddr, const unsigned* v) {
   asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};"
                :: "r"(taddr), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]) : "memory");
+}
+__device__ __forceinline__ void st_x16(unsigned taddr, const unsigned* v) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};"
+               :: "r"(taddr), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
+                  "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]) : "memory");
 }
 __device__ __forceinline__ void st_wait() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void ld_x8(unsigned taddr, unsigned* v) {
@@ -1329,13 +1342,32 @@ class _TC:
     self.close()
     self.w('unsigned hv[16], lv[16];')
     self.w('#pragma unroll')
-    self.w('for (int i = 0; i < 16; ++i) { hv[i] = tfb_tc::tf32_rna(u[i]); lv[i] = __float_as_uint(u[i] - __uint_as_float(hv[i])); }')
-    self.w('tfb_tc::st_x8(slot + c0, hv);')
-    self.w(f'tfb_tc::st_x8(slot + {half}u + c0, lv);')
-    self.open(f'if (c0 + 8u < {kp}u)')
-    self.w('tfb_tc::st_x8(slot + c0 + 8u, hv + 8);')
-    self.w(f'tfb_tc::st_x8(slot + {half}u + c0 + 8u, lv + 8);')
-    self.close()
+    if int(self.plan.params.get('lpk', 0)):
+      # lo = u - hi as packed FMAs (exact), 16 columns per tensor-memory store
+      self.open('for (int p = 0; p < 8; ++p)')
+      self.w('hv[2 * p] = tfb_tc::tf32_rna(u[2 * p]);')
+      self.w('hv[2 * p + 1] = tfb_tc::tf32_rna(u[2 * p + 1]);')
+      self.w('const float2 lo = __ffma2_rn(make_float2(__uint_as_float(hv[2 * p]), __uint_as_float(hv[2 * p + 1])), '
+             'make_float2(-1.0f, -1.0f), make_float2(u[2 * p], u[2 * p + 1]));')
+      self.w('lv[2 * p] = __float_as_uint(lo.x);')
+      self.w('lv[2 * p + 1] = __float_as_uint(lo.y);')
+      self.close()
+      self.open(f'if (c0 + 8u < {kp}u)')
+      self.w('tfb_tc::st_x16(slot + c0, hv);')
+      self.w(f'tfb_tc::st_x16(slot + {half}u + c0, lv);')
+      self.close()
+      self.open('else')
+      self.w('tfb_tc::st_x8(slot + c0, hv);')
+      self.w(f'tfb_tc::st_x8(slot + {half}u + c0, lv);')
+      self.close()
+    else:
+      self.w('for (int i = 0; i < 16; ++i) { hv[i] = tfb_tc::tf32_rna(u[i]); lv[i] = __float_as_uint(u[i] - __uint_as_float(hv[i])); }')
+      self.w('tfb_tc::st_x8(slot + c0, hv);')
+      self.w(f'tfb_tc::st_x8(slot + {half}u + c0, lv);')
+      self.open(f'if (c0 + 8u < {kp}u)')
+      self.w('tfb_tc::st_x8(slot + c0 + 8u, hv + 8);')
+      self.w(f'tfb_tc::st_x8(slot + {half}u + c0 + 8u, lv + 8);')
+      self.close()
     self.close()
     self.w('tfb_tc::st_wait();')
     self.w('tfb_tc::fence_before();')
@@ -1854,7 +1886,13 @@ class _TC:
         self.w(f'tfb_tc::ld_x8(dm + {n_mma + 8 * k}u, dc + {8 * i});')
       self.w('tfb_tc::ld_wait();')
       self.w('#pragma unroll')
-      self.w(f'for (int i = 0; i < {8 * len(ks)}; ++i) acc[{8 * k0} + i] = __uint_as_float(dv[i]) + __uint_as_float(dc[i]);')
+      if int(self.plan.params.get('epk', 0)):
+        self.w(f'for (int i = 0; i < {4 * len(ks)}; ++i) {{ const float2 v = __fadd2_rn('
+               'make_float2(__uint_as_float(dv[2 * i]), __uint_as_float(dv[2 * i + 1])), '
+               'make_float2(__uint_as_float(dc[2 * i]), __uint_as_float(dc[2 * i + 1]))); '
+               f'acc[{8 * k0} + 2 * i] = v.x; acc[{8 * k0} + 2 * i + 1] = v.y; }}')
+      else:
+        self.w(f'for (int i = 0; i < {8 * len(ks)}; ++i) acc[{8 * k0} + i] = __uint_as_float(dv[i]) + __uint_as_float(dc[i]);')
       self.close()
     self.w('tfb_tc::fence_before();')
     self.w(f'tfb_tc::mbar_arrive(&bars[{self.BAR["dfree"]}u + db]);')
