@@ -609,6 +609,7 @@ def impl_ours(args, rank, world, dist):
              'tf32x3_estg': {'precision': 'tf32x3', 'variant': {'form': 'u', 'estg': 1}},
              'tf32x3_nlpk': {'precision': 'tf32x3', 'variant': {'form': 'u', 'lpk': 0}},
              'tf32x3_nepk': {'precision': 'tf32x3', 'variant': {'form': 'u', 'epk': 0}},
+             'tf32x3_sl3': {'precision': 'tf32x3', 'variant': {'form': 'u', 'sleep': 3}},
 
              'plain_rs2': {'variant': {'strategy': 'colprog', 'threads': 256, 'rsplit': 2, 'min_blocks': 2}},
              'tf32x3_form_b': {'precision': 'tf32x3', 'variant': {'form': 'b'}},

@@ -382,13 +382,15 @@ def plan(chain, shape, precision, variant):
   if (int(variant.get('urows', 2 if pipe == 3 else 1)) == 2 and pipe in (2, 3) and not direct
       and all(t.K % 2 == 0 for t in shape.terms)):
     params['urows'] = 2
-  if pipe == 3 and int(variant.get('sleep', 3)):
+  if pipe == 3 and int(variant.get('sleep', 4)):
     # waiting threads sleep in try_wait (global-timer bound) instead of spinning, leaving
     # the issue slots to the producers (order-6 chain, 500,000 elements: 6.51e8 el/s with
-    # every role sleeping against 6.45e8 spinning); the default 3 keeps the MMA thread
-    # spinning, so it issues as soon as a lane phase arrives (6.61e8 against 6.58e8 with
-    # every role sleeping and 6.46e8 with the producers spinning too, option 2)
-    params['sleep'] = int(variant.get('sleep', 3))
+    # every role sleeping against 6.45e8 spinning); 3 keeps the MMA thread spinning, so it
+    # issues as soon as a lane phase arrives (6.61e8 against 6.58e8 with every role
+    # sleeping and 6.46e8 with the producers spinning too, option 2); the default 4 also
+    # lets the producers poll 32 times before they sleep, so a phase that completes soon
+    # costs no wake-up (6.93e8 against 6.79e8 with option 3)
+    params['sleep'] = int(variant.get('sleep', 4))
   if opad:
     # option: output staging rows padded by 16 bytes (no bank conflicts on the staging
     # stores), each row written by its own bulk copy (measured slower: 6.44e8 el/s against
@@ -477,6 +479,18 @@ __device__ __forceinline__ bool mbar_wait_s(uint64_t* bar, unsigned parity, unsi
     if (t0 == 0) t0 = t;
     else if (t - t0 > limit_ns) return false;
   }
+}
+// a few polls without a suspend hint first (a phase that completes within them costs no
+// wake-up), then the sleeping wait
+__device__ __forceinline__ bool mbar_wait_h(uint64_t* bar, unsigned parity, unsigned long long limit_ns) {
+  const unsigned addr = smem_u32(bar);
+  for (int i = 0; i < 32; ++i) {
+    unsigned ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok) : "r"(addr), "r"(parity) : "memory");
+    if (ok) return true;
+  }
+  return mbar_wait_s(bar, parity, limit_ns);
 }
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -734,11 +748,12 @@ class _TC:
     lim = self.WAIT_NS if sleep else self.WAIT_LIMIT
     # which roles sleep: 1 all; 2 the epilogue and loader warps (the producers and the MMA
     # thread spin); 3 all but the MMA thread
-    spin_roles = {2: ('mma', 'producers'), 3: ('mma',)}.get(sleep, ())
+    spin_roles = {2: ('mma', 'producers'), 3: ('mma',), 4: ('mma',)}.get(sleep, ())
+    hybrid_roles = {4: ('producers',)}.get(sleep, ())
 
     def role(name):
       spin = name in spin_roles or not sleep
-      self.wfn = 'mbar_wait' if spin else 'mbar_wait_s'
+      self.wfn = 'mbar_wait' if spin else ('mbar_wait_h' if name in hybrid_roles else 'mbar_wait_s')
       return self.WAIT_LIMIT if spin else self.WAIT_NS
     # loader warp: 1 fetches all inputs of the next tile, 2 only the bulk copy of the B
     # blocks (the producers keep issuing the small R copies)

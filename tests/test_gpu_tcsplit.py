@@ -128,7 +128,7 @@ PIPE3_OPTIONS = [{'form': 'u', 'qreg': 1}, {'form': 'u', 'slots': 2}, {'form': '
                  {'form': 'u', 'direct': 1}, {'form': 'u', 'l64': 1},
                  {'form': 'u', 'oswz': 1}, {'form': 'u', 'estg': 1},
                  {'form': 'u', 'sleep': 1}, {'form': 'u', 'sleep': 2}, {'form': 'u', 'lpk': 0},
-                 {'form': 'u', 'epk': 0}]
+                 {'form': 'u', 'epk': 0}, {'form': 'u', 'sleep': 3}]
 
 
 @pytest.mark.parametrize('variant', PIPE3_OPTIONS, ids=lambda v: ','.join(f'{k}={x}' for k, x in v.items() if k != 'form'))
